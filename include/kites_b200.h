@@ -1,0 +1,245 @@
+/*
+ * kites_b200.h -- C ABI of the B200 vertex-centric engine.
+ *
+ * Plain pointers and sizes only; every call returns a kites_status (0 = ok)
+ * and leaves a message for kites_last_error_string() on failure.  The C++
+ * front-end in include/kites/ (the drop-in for farkhor/KiTES's API) calls
+ * these entry points and turns a non-zero status into std::runtime_error,
+ * as the reference's CUDAErrorCheck does (kites/common/cuda_error_check.cuh:9-18).
+ *
+ * Each declaration names the reference interface it replaces
+ * (paths relative to the KiTES project root).
+ */
+#ifndef KITES_B200_H_
+#define KITES_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define KITES_B200_ABI_VERSION 1
+
+typedef enum kites_status {
+  KITES_OK = 0,
+  KITES_ERR_INVALID = 1,       /* bad argument / size / vpg not a power of 2 */
+  KITES_ERR_OOM = 2,           /* device or pinned allocation failed         */
+  KITES_ERR_CUDA = 3,          /* a CUDA runtime call failed                  */
+  KITES_ERR_TIMEOUT = 4,       /* iteration limit or bounded wait exhausted   */
+  KITES_ERR_UNSUPPORTED = 5,   /* operator/strategy combination not offered   */
+  KITES_ERR_NO_DEVICE = 6      /* no CUDA device / not an sm_100 part         */
+} kites_status;
+
+/* Built-in vertex programs.  Each one is a set of the reference's four user
+ * functions (README.md:14-24) with a precompiled sm_100a kernel:
+ *   SSSP       init copy, partial = src + w saturating at 0xFFFFFFFF, min, <
+ *   SSSP_WRAP  same with u32 wrap-around add (the example's lambda verbatim,
+ *              examples/sssp_basic_single_device.cu:42-43)
+ *   BFS        partial = src + 1 saturating, min, <
+ *   CC         partial = src (min label), min, <
+ *   PAGERANK   FP32, 20 synchronous (Jacobi) iterations by default          */
+typedef enum kites_op {
+  KITES_OP_SSSP = 0,
+  KITES_OP_SSSP_WRAP = 1,
+  KITES_OP_BFS = 2,
+  KITES_OP_CC = 3,
+  KITES_OP_PAGERANK = 4
+} kites_op;
+
+/* Per-iteration traversal strategies.  PLAIN is the pull iteration over the
+ * bitmap frontier (kites/device/kernels_single_device.cuh:18-426 re-designed);
+ * AUTO lets the learned selector pick per iteration, falling back to PLAIN
+ * when the predicted gain is under the margin.  The others force one
+ * strategy for every iteration (used to record training timings). */
+typedef enum kites_strategy {
+  KITES_STRATEGY_PLAIN = 0,
+  KITES_STRATEGY_AUTO = 1,
+  KITES_STRATEGY_PUSH = 2,      /* push over the compacted changed queue     */
+  KITES_STRATEGY_PULL_ALL = 3,  /* dense pull sweep over every vertex        */
+  KITES_STRATEGY_TPV1 = 4,      /* pull, 1 thread per active vertex          */
+  KITES_STRATEGY_TPV4 = 5,      /* pull, 4 threads per active vertex         */
+  KITES_STRATEGY_TPV8 = 6,      /* pull, 8 threads per active vertex         */
+  KITES_STRATEGY_TPV32 = 7,     /* pull, one warp per active vertex          */
+  KITES_STRATEGY_COUNT = 8
+} kites_strategy;
+
+typedef struct kites_engine kites_engine;
+typedef struct kites_graph kites_graph;
+
+/* A host- or device-resident CSC graph as kites::graph_csr holds it
+ * (kites/graph/graph_csr.h:28-39): rows are destinations, col_indices are
+ * the sources of each row's in-edges sorted ascending.  Exactly one of
+ * row_offsets / row_offsets32 is non-NULL; likewise for the out-adjacency.
+ * If out_col_indices is NULL and vertex_per_group == 1 the engine derives
+ * the out-adjacency from the CSC itself. */
+typedef struct kites_csc_view {
+  uint64_t n_vertices;              /* rows; engine pads to a multiple of 128 */
+  uint64_t n_edges;
+  const uint64_t *row_offsets;      /* R  [n_vertices + 1]                    */
+  const uint32_t *row_offsets32;
+  const uint32_t *col_indices;      /* C  [n_edges]                           */
+  const void *edge_values;          /* E  [n_edges] x edge_value_size, or NULL */
+  uint32_t edge_value_size;         /* bytes per edge value (0 if none)       */
+  uint32_t vertex_value_size;       /* bytes per vertex value                 */
+  const void *vertex_values;        /* V  [n_vertices] initial values or NULL */
+  uint32_t vertex_per_group;        /* vpg, a power of two                    */
+  int32_t directed;                 /* kites::graph_property::directed == 1   */
+  const uint32_t *frontier_bits;    /* vBitmap words (LSB = lowest id) or NULL */
+  uint64_t frontier_nbits;          /* bits in vBitmap                        */
+  uint64_t n_out_rows;              /* dir_R entries - 1                      */
+  const uint64_t *out_row_offsets;  /* dir_R                                  */
+  const uint32_t *out_row_offsets32;
+  const uint32_t *out_col_indices;  /* dir_C                                  */
+  uint64_t n_out_edges;
+  int32_t on_device;                /* 1 if every pointer above is device memory */
+} kites_csc_view;
+
+/* Device pointers of an uploaded graph, for the header-side generic kernels
+ * (the C++ front-end instantiates user lambdas in the caller's TU). */
+typedef struct kites_device_view {
+  uint64_t n_vertices;              /* padded */
+  uint64_t n_edges;
+  uint64_t nbits;                   /* frontier bits (vertices or groups) */
+  uint32_t vertex_per_group;
+  int32_t directed;
+  int32_t offsets64;                /* 1 if row arrays are uint64 */
+  void *V;
+  const void *R;
+  const uint32_t *C;
+  void *E;
+  const void *dir_R;
+  const uint32_t *dir_C;
+  uint32_t *frontier[2];            /* even / odd bitmaps */
+  uint32_t *update_flag;            /* one device word */
+  void *stream;                     /* cudaStream_t the engine works on */
+} kites_device_view;
+
+typedef struct kites_run_opts {
+  int32_t strategy;                 /* kites_strategy */
+  int32_t device_loop;              /* 1: iteration loop captured in a CUDA
+                                       graph with device-side convergence;
+                                       0: host loop, flag read back per trip
+                                       (compute.cuh:57-128)                  */
+  uint64_t max_iterations;          /* 0 = until convergence                */
+  uint32_t pagerank_iterations;     /* PAGERANK only (default 20)           */
+  float damping;                    /* PAGERANK only (default 0.85)         */
+  float selector_margin;            /* AUTO: min predicted gain (fraction)  */
+  int32_t record_iterations;        /* fill kites_run_stats.iter_* arrays   */
+  int32_t time_kernels;             /* host loop with CUDA events around each
+                                       pull launch (fills pull_kernel_*)    */
+} kites_run_opts;
+
+#define KITES_MAX_RECORDED_ITERS 4096
+
+typedef struct kites_run_stats {
+  uint64_t iterations;              /* kernel iterations, as compute.cuh:135 counts */
+  double device_ms;                 /* CUDA-event time of the iteration loop */
+  double host_ms;                   /* wall time of the whole call           */
+  uint64_t edges_traversed;         /* sum over iterations of in-edges of active vertices */
+  uint64_t algorithmic_bytes;       /* sum over iterations of B_t            */
+  uint64_t strategy_hist[KITES_STRATEGY_COUNT];
+  uint64_t kernel_launches;         /* engine kernels launched by the call   */
+  double pull_kernel_ms;            /* time_kernels: summed pull-kernel time */
+  uint64_t pull_kernel_launches;
+  uint64_t pull_kernel_bytes;       /* algorithmic bytes of those launches   */
+  uint32_t n_recorded;
+  uint8_t iter_strategy[KITES_MAX_RECORDED_ITERS];
+  float iter_ms[KITES_MAX_RECORDED_ITERS];
+  uint64_t iter_active[KITES_MAX_RECORDED_ITERS];
+  uint64_t iter_edges[KITES_MAX_RECORDED_ITERS];
+} kites_run_stats;
+
+/* ---- library / engine ------------------------------------------------ */
+
+/* Message of the last failed call on this host thread ("" if none). */
+const char *kites_last_error_string(void);
+int kites_abi_version(void);
+void kites_default_run_opts(kites_run_opts *opts);
+
+/* Replaces kites::nv_gpu(int) (kites/device/nv_gpu.cuh:32-37): binds the
+ * device, creates the engine's streams and its pooled allocator. */
+int kites_engine_create(int device, kites_engine **out);
+int kites_engine_destroy(kites_engine *eng);
+/* Replaces nv_gpu::queryMemUsage (nv_gpu.cuh:78-86), in bytes. */
+int kites_engine_mem_usage(kites_engine *eng, uint64_t *used, uint64_t *total,
+                           uint64_t *pool_reserved);
+int kites_engine_sync(kites_engine *eng);  /* nv_gpu::sync (nv_gpu.cuh:45-48) */
+
+/* ---- graphs ----------------------------------------------------------- */
+
+/* Replaces kites::make_graph_csr_for_device / graph_csr_device's constructor
+ * (kites/graph/graph_csr_device.cuh:83-152): copies the CSC, the initial
+ * values and the initial frontier to the device and builds the engine's
+ * B200 layout (edge-balanced chunk table, weighted out-CSR). */
+int kites_graph_upload(kites_engine *eng, const kites_csc_view *view,
+                       kites_graph **out);
+int kites_graph_destroy(kites_graph *g);
+int kites_graph_device_view(kites_graph *g, kites_device_view *out);
+/* Copy vertex values in or out (host or device pointer, cudaMemcpyDefault),
+ * as host_pinned_buffer<vT>(devGrph.V) does (host_pinned_buffer.cuh:52-57). */
+int kites_graph_get_values(kites_graph *g, void *dst, uint64_t n_vertices);
+int kites_graph_set_values(kites_graph *g, const void *src, uint64_t n_vertices);
+int kites_graph_set_frontier(kites_graph *g, const uint32_t *bits, uint64_t nbits);
+
+/* ---- runs --------------------------------------------------------------- */
+
+/* kites::process<launch::sync>(devGrph, dev, initF, nbrCompF, redF, updF)
+ * (kites/device/compute.cuh:29-137) for a built-in operator: iterates the
+ * graph's own vertex values from its current frontier to the fixed point,
+ * in place, on the device. */
+int kites_process(kites_engine *eng, kites_graph *g, int op,
+                  const kites_run_opts *opts, kites_run_stats *stats);
+
+/* Single-source SSSP/BFS from `source`: sets V = INF except V[source] = 0 and
+ * the frontier to source's out-neighbours (the example's pre-processing,
+ * examples/sssp_basic_single_device.cu:9-27), runs kites_process, and copies
+ * the distances to `dist_out` (host or device) if it is non-NULL. */
+int kites_sssp(kites_engine *eng, kites_graph *g, int op, uint32_t source,
+               uint32_t *dist_out, const kites_run_opts *opts,
+               kites_run_stats *stats);
+
+/* Batched multi-source SSSP/BFS: K sources at once, distances in a
+ * V x K vertex-major array (dist_out[v*K + k]); K <= 64. */
+int kites_sssp_batch(kites_engine *eng, kites_graph *g, int op,
+                     const uint32_t *sources, uint32_t k, uint32_t *dist_out,
+                     const kites_run_opts *opts, kites_run_stats *stats);
+
+/* Min-label connected components: V[v] = v, every vertex active. */
+int kites_cc(kites_engine *eng, kites_graph *g, uint32_t *labels_out,
+             const kites_run_opts *opts, kites_run_stats *stats);
+
+/* FP32 PageRank, `opts->pagerank_iterations` Jacobi steps of
+ * PR <- (1-d)/n_real + d * sum PR(u)/outdeg(u), uniform 1/n_real start. */
+int kites_pagerank(kites_engine *eng, kites_graph *g, uint64_t n_real,
+                   float *rank_out, const kites_run_opts *opts,
+                   kites_run_stats *stats);
+
+/* ---- synthetic graphs (host, deterministic, OpenMP) ------------------ */
+
+/* Candidate edges come from a counter-based SplitMix64 stream; self-loops,
+ * out-of-range ids (n_vertices < 2^scale) and duplicate pairs are dropped
+ * and the list is topped up from further candidates until n_edges remain.
+ * Output is in candidate order.  Weights uniform in [w_lo, w_hi]. */
+int kites_gen_rmat(uint32_t scale, uint64_t n_vertices, uint64_t n_edges,
+                   double a, double b, double c, uint64_t seed, uint32_t w_lo,
+                   uint32_t w_hi, uint32_t *src, uint32_t *dst, uint32_t *w);
+int kites_gen_er(uint64_t n_vertices, uint64_t n_edges, uint64_t seed,
+                 uint32_t w_lo, uint32_t w_hi, uint32_t *src, uint32_t *dst,
+                 uint32_t *w);
+/* side x side 4-neighbour grid, both directions, 2*2*side*(side-1) edges. */
+int kites_gen_grid(uint32_t side, uint64_t seed, uint32_t w_lo, uint32_t w_hi,
+                   uint32_t *src, uint32_t *dst, uint32_t *w);
+/* Edge list -> CSC keyed by destination, rows sorted by source (ties in
+ * input order), graph_raw.h:102,131 semantics; R has n_vertices+1 entries. */
+int kites_csc_from_edges(uint64_t n_vertices, uint64_t n_edges,
+                         const uint32_t *src, const uint32_t *dst,
+                         const uint32_t *w, uint64_t *R, uint32_t *C,
+                         uint32_t *E);
+
+#ifdef __cplusplus
+}  /* extern "C" */
+#endif
+
+#endif /* KITES_B200_H_ */

@@ -1,0 +1,394 @@
+"""ctypes binding of include/kites_b200.h (libkites_b200.so, built in-tree).
+
+This is how Python callers -- the parity tests, bench.py, smoke() -- reach
+the engine: through the same C ABI the C++ front-end in include/kites/
+uses.  There is no fallback: if the shared library is missing,
+``load()`` raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from ctypes import (POINTER, Structure, c_char_p, c_double, c_float, c_int,
+                    c_int32, c_uint8, c_uint32, c_uint64, c_void_p)
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libkites_b200.so")
+
+OK, ERR_INVALID, ERR_OOM, ERR_CUDA, ERR_TIMEOUT, ERR_UNSUPPORTED, ERR_NO_DEVICE = range(7)
+OP_SSSP, OP_SSSP_WRAP, OP_BFS, OP_CC, OP_PAGERANK = range(5)
+(STRATEGY_PLAIN, STRATEGY_AUTO, STRATEGY_PUSH, STRATEGY_PULL_ALL, STRATEGY_TPV1,
+ STRATEGY_TPV4, STRATEGY_TPV8, STRATEGY_TPV32) = range(8)
+STRATEGY_COUNT = 8
+MAX_RECORDED_ITERS = 4096
+INF = 0xFFFFFFFF
+
+# Every symbol include/kites_b200.h declares.
+EXPORTED = [
+    "kites_last_error_string", "kites_abi_version", "kites_default_run_opts",
+    "kites_engine_create", "kites_engine_destroy", "kites_engine_mem_usage",
+    "kites_engine_sync", "kites_graph_upload", "kites_graph_destroy",
+    "kites_graph_device_view", "kites_graph_get_values", "kites_graph_set_values",
+    "kites_graph_set_frontier", "kites_process", "kites_sssp", "kites_sssp_batch",
+    "kites_cc", "kites_pagerank", "kites_gen_rmat", "kites_gen_er", "kites_gen_grid",
+    "kites_csc_from_edges",
+]
+
+
+class CscView(Structure):
+    _fields_ = [
+        ("n_vertices", c_uint64), ("n_edges", c_uint64),
+        ("row_offsets", c_void_p), ("row_offsets32", c_void_p),
+        ("col_indices", c_void_p), ("edge_values", c_void_p),
+        ("edge_value_size", c_uint32), ("vertex_value_size", c_uint32),
+        ("vertex_values", c_void_p), ("vertex_per_group", c_uint32),
+        ("directed", c_int32), ("frontier_bits", c_void_p),
+        ("frontier_nbits", c_uint64), ("n_out_rows", c_uint64),
+        ("out_row_offsets", c_void_p), ("out_row_offsets32", c_void_p),
+        ("out_col_indices", c_void_p), ("n_out_edges", c_uint64),
+        ("on_device", c_int32),
+    ]
+
+
+class DeviceView(Structure):
+    _fields_ = [
+        ("n_vertices", c_uint64), ("n_edges", c_uint64), ("nbits", c_uint64),
+        ("vertex_per_group", c_uint32), ("directed", c_int32), ("offsets64", c_int32),
+        ("V", c_void_p), ("R", c_void_p), ("C", c_void_p), ("E", c_void_p),
+        ("dir_R", c_void_p), ("dir_C", c_void_p), ("frontier", c_void_p * 2),
+        ("update_flag", c_void_p), ("stream", c_void_p),
+    ]
+
+
+class RunOpts(Structure):
+    _fields_ = [
+        ("strategy", c_int32), ("device_loop", c_int32),
+        ("max_iterations", c_uint64), ("pagerank_iterations", c_uint32),
+        ("damping", c_float), ("selector_margin", c_float),
+        ("record_iterations", c_int32), ("time_kernels", c_int32),
+    ]
+
+
+class RunStats(Structure):
+    _fields_ = [
+        ("iterations", c_uint64), ("device_ms", c_double), ("host_ms", c_double),
+        ("edges_traversed", c_uint64), ("algorithmic_bytes", c_uint64),
+        ("strategy_hist", c_uint64 * STRATEGY_COUNT), ("kernel_launches", c_uint64),
+        ("pull_kernel_ms", c_double), ("pull_kernel_launches", c_uint64),
+        ("pull_kernel_bytes", c_uint64),
+        ("n_recorded", c_uint32),
+        ("iter_strategy", c_uint8 * MAX_RECORDED_ITERS),
+        ("iter_ms", c_float * MAX_RECORDED_ITERS),
+        ("iter_active", c_uint64 * MAX_RECORDED_ITERS),
+        ("iter_edges", c_uint64 * MAX_RECORDED_ITERS),
+    ]
+
+
+class KitesError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"kites status {status}: {msg}")
+        self.status = status
+
+
+_lib = None
+
+
+def load(path: str = LIB_PATH):
+    """Load the in-tree shared library (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise ImportError(f"{path} is missing; run `python -m kites_b200.build`")
+    lib = ctypes.CDLL(path)
+    vp, u32, u64 = c_void_p, c_uint32, c_uint64
+    sigs = {
+        "kites_last_error_string": (c_char_p, []),
+        "kites_abi_version": (c_int, []),
+        "kites_default_run_opts": (None, [POINTER(RunOpts)]),
+        "kites_engine_create": (c_int, [c_int, POINTER(c_void_p)]),
+        "kites_engine_destroy": (c_int, [vp]),
+        "kites_engine_mem_usage": (c_int, [vp, POINTER(c_uint64), POINTER(c_uint64),
+                                           POINTER(c_uint64)]),
+        "kites_engine_sync": (c_int, [vp]),
+        "kites_graph_upload": (c_int, [vp, POINTER(CscView), POINTER(c_void_p)]),
+        "kites_graph_destroy": (c_int, [vp]),
+        "kites_graph_device_view": (c_int, [vp, POINTER(DeviceView)]),
+        "kites_graph_get_values": (c_int, [vp, vp, u64]),
+        "kites_graph_set_values": (c_int, [vp, vp, u64]),
+        "kites_graph_set_frontier": (c_int, [vp, vp, u64]),
+        "kites_process": (c_int, [vp, vp, c_int, POINTER(RunOpts), POINTER(RunStats)]),
+        "kites_sssp": (c_int, [vp, vp, c_int, u32, vp, POINTER(RunOpts),
+                               POINTER(RunStats)]),
+        "kites_sssp_batch": (c_int, [vp, vp, c_int, vp, u32, vp, POINTER(RunOpts),
+                                     POINTER(RunStats)]),
+        "kites_cc": (c_int, [vp, vp, vp, POINTER(RunOpts), POINTER(RunStats)]),
+        "kites_pagerank": (c_int, [vp, vp, u64, vp, POINTER(RunOpts), POINTER(RunStats)]),
+        "kites_gen_rmat": (c_int, [u32, u64, u64, c_double, c_double, c_double, u64,
+                                   u32, u32, vp, vp, vp]),
+        "kites_gen_er": (c_int, [u64, u64, u64, u32, u32, vp, vp, vp]),
+        "kites_gen_grid": (c_int, [u32, u64, u32, u32, vp, vp, vp]),
+        "kites_csc_from_edges": (c_int, [u64, u64, vp, vp, vp, vp, vp, vp]),
+    }
+    for name, (res, args) in sigs.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _check(status):
+    if status != OK:
+        msg = load().kites_last_error_string().decode(errors="replace")
+        raise KitesError(status, msg)
+
+
+def _p(a):
+    """Pointer of a numpy array, a torch tensor, or None."""
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data_as(c_void_p)
+    if hasattr(a, "data_ptr"):
+        return c_void_p(a.data_ptr())
+    if isinstance(a, int):
+        return c_void_p(a)
+    raise TypeError(type(a))
+
+
+def default_opts(**kw) -> RunOpts:
+    o = RunOpts()
+    load().kites_default_run_opts(ctypes.byref(o))
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
+# ---------------------------------------------------------------------------
+# Objects
+# ---------------------------------------------------------------------------
+
+class Engine:
+    """One GPU (the reference's kites::nv_gpu, kites/device/nv_gpu.cuh:21-88)."""
+
+    def __init__(self, device: int = 0):
+        self._h = c_void_p()
+        _check(load().kites_engine_create(device, ctypes.byref(self._h)))
+        self.device = device
+
+    def close(self):
+        if self._h:
+            load().kites_engine_destroy(self._h)
+            self._h = c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def mem_usage(self):
+        used, total, pool = c_uint64(), c_uint64(), c_uint64()
+        _check(load().kites_engine_mem_usage(self._h, ctypes.byref(used),
+                                             ctypes.byref(total), ctypes.byref(pool)))
+        return used.value, total.value, pool.value
+
+    def sync(self):
+        _check(load().kites_engine_sync(self._h))
+
+
+class Graph:
+    """A device-resident graph (kites::graph_csr_device)."""
+
+    def __init__(self, engine: Engine, R, C, E=None, V=None, frontier=None,
+                 frontier_nbits=0, vpg=1, directed=True, dir_R=None, dir_C=None,
+                 on_device=False, n_vertices=None, n_edges=None,
+                 vertex_value_size=4):
+        self.engine = engine
+        v = CscView()
+        if on_device:
+            v.n_vertices = int(n_vertices)
+            v.n_edges = int(n_edges)
+            r_is64 = R.dtype.itemsize == 8 if hasattr(R, "dtype") else True
+        else:
+            R = np.ascontiguousarray(R)
+            C = np.ascontiguousarray(C, dtype=np.uint32)
+            v.n_vertices = R.shape[0] - 1
+            v.n_edges = C.shape[0]
+            r_is64 = R.dtype.itemsize == 8
+            if E is not None:
+                E = np.ascontiguousarray(E)
+            if V is not None:
+                V = np.ascontiguousarray(V)
+            if frontier is not None:
+                frontier = np.ascontiguousarray(frontier, dtype=np.uint32)
+            if dir_R is not None:
+                dir_R = np.ascontiguousarray(dir_R)
+                dir_C = np.ascontiguousarray(dir_C, dtype=np.uint32)
+        if r_is64:
+            v.row_offsets = _p(R)
+        else:
+            v.row_offsets32 = _p(R)
+        v.col_indices = _p(C)
+        v.edge_values = _p(E)
+        v.edge_value_size = 0 if E is None else 4
+        v.vertex_value_size = vertex_value_size
+        v.vertex_values = _p(V)
+        v.vertex_per_group = vpg
+        v.directed = 1 if directed else 0
+        v.frontier_bits = _p(frontier)
+        v.frontier_nbits = int(frontier_nbits)
+        if dir_R is not None:
+            v.n_out_rows = dir_R.shape[0] - 1
+            if dir_R.dtype.itemsize == 8:
+                v.out_row_offsets = _p(dir_R)
+            else:
+                v.out_row_offsets32 = _p(dir_R)
+            v.out_col_indices = _p(dir_C)
+            v.n_out_edges = dir_C.shape[0]
+        v.on_device = 1 if on_device else 0
+        self._keep = (R, C, E, V, frontier, dir_R, dir_C)
+        self._h = c_void_p()
+        _check(load().kites_graph_upload(engine._h, ctypes.byref(v), ctypes.byref(self._h)))
+        self._keep = None
+        self.n_vertices = int(v.n_vertices)
+        self.n_edges = int(v.n_edges)
+        dv = self.device_view()
+        self.n_padded = int(dv.n_vertices)
+
+    def close(self):
+        if self._h:
+            load().kites_graph_destroy(self._h)
+            self._h = c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def device_view(self) -> DeviceView:
+        dv = DeviceView()
+        _check(load().kites_graph_device_view(self._h, ctypes.byref(dv)))
+        return dv
+
+    def get_values(self, n=None, dtype=np.uint32):
+        n = self.n_padded if n is None else n
+        out = np.empty(n, dtype=dtype)
+        _check(load().kites_graph_get_values(self._h, _p(out), n))
+        return out
+
+    def set_values(self, values):
+        values = np.ascontiguousarray(values)
+        _check(load().kites_graph_set_values(self._h, _p(values), values.shape[0]))
+
+    def set_frontier(self, bits, nbits):
+        bits = np.ascontiguousarray(bits, dtype=np.uint32)
+        _check(load().kites_graph_set_frontier(self._h, _p(bits), nbits))
+
+    # ---- runs ----
+    def process(self, op, opts=None):
+        st = RunStats()
+        o = opts or default_opts()
+        _check(load().kites_process(self.engine._h, self._h, op, ctypes.byref(o),
+                                    ctypes.byref(st)))
+        return st
+
+    def sssp(self, source, op=OP_SSSP, out=None, opts=None):
+        """out=None: new host array; out=False: leave the distances on the
+        device (graph values); otherwise a host/device buffer of n values."""
+        st = RunStats()
+        o = opts or default_opts()
+        if out is None:
+            out = np.empty(self.n_vertices, dtype=np.uint32)
+        ptr = None if out is False else _p(out)
+        _check(load().kites_sssp(self.engine._h, self._h, op, source, ptr,
+                                 ctypes.byref(o), ctypes.byref(st)))
+        return (None if out is False else out), st
+
+    def sssp_batch(self, sources, op=OP_SSSP, out=None, opts=None):
+        st = RunStats()
+        o = opts or default_opts()
+        src = np.ascontiguousarray(sources, dtype=np.uint32)
+        k = src.shape[0]
+        if out is None:
+            out = np.empty((self.n_vertices, k), dtype=np.uint32)
+        _check(load().kites_sssp_batch(self.engine._h, self._h, op, _p(src), k, _p(out),
+                                       ctypes.byref(o), ctypes.byref(st)))
+        return out, st
+
+    def cc(self, out=None, opts=None):
+        st = RunStats()
+        o = opts or default_opts()
+        if out is None:
+            out = np.empty(self.n_vertices, dtype=np.uint32)
+        _check(load().kites_cc(self.engine._h, self._h, _p(out), ctypes.byref(o),
+                               ctypes.byref(st)))
+        return out, st
+
+    def pagerank(self, n_real=None, iterations=20, damping=0.85, out=None, opts=None):
+        st = RunStats()
+        o = opts or default_opts()
+        o.pagerank_iterations = iterations
+        o.damping = damping
+        n_real = self.n_vertices if n_real is None else n_real
+        if out is None:
+            out = np.empty(n_real, dtype=np.float32)
+        _check(load().kites_pagerank(self.engine._h, self._h, n_real, _p(out),
+                                     ctypes.byref(o), ctypes.byref(st)))
+        return out, st
+
+
+# ---------------------------------------------------------------------------
+# Synthetic graphs (host)
+# ---------------------------------------------------------------------------
+
+def gen_rmat(scale, n_edges, a=0.57, b=0.19, c=0.19, seed=1, w_lo=1, w_hi=255,
+             n_vertices=0):
+    src = np.empty(n_edges, dtype=np.uint32)
+    dst = np.empty(n_edges, dtype=np.uint32)
+    w = np.empty(n_edges, dtype=np.uint32)
+    _check(load().kites_gen_rmat(scale, n_vertices, n_edges, a, b, c, seed, w_lo, w_hi,
+                                 _p(src), _p(dst), _p(w)))
+    return src, dst, w
+
+
+def gen_er(n_vertices, n_edges, seed=1, w_lo=1, w_hi=255):
+    src = np.empty(n_edges, dtype=np.uint32)
+    dst = np.empty(n_edges, dtype=np.uint32)
+    w = np.empty(n_edges, dtype=np.uint32)
+    _check(load().kites_gen_er(n_vertices, n_edges, seed, w_lo, w_hi, _p(src), _p(dst),
+                               _p(w)))
+    return src, dst, w
+
+
+def gen_grid(side, seed=1, w_lo=1, w_hi=1000):
+    m = 4 * side * (side - 1)
+    src = np.empty(m, dtype=np.uint32)
+    dst = np.empty(m, dtype=np.uint32)
+    w = np.empty(m, dtype=np.uint32)
+    _check(load().kites_gen_grid(side, seed, w_lo, w_hi, _p(src), _p(dst), _p(w)))
+    return src, dst, w
+
+
+def csc_from_edges(n_vertices, src, dst, w=None):
+    src = np.ascontiguousarray(src, dtype=np.uint32)
+    dst = np.ascontiguousarray(dst, dtype=np.uint32)
+    m = src.shape[0]
+    R = np.empty(n_vertices + 1, dtype=np.uint64)
+    C = np.empty(m, dtype=np.uint32)
+    E = np.empty(m, dtype=np.uint32) if w is not None else None
+    if w is not None:
+        w = np.ascontiguousarray(w, dtype=np.uint32)
+    _check(load().kites_csc_from_edges(n_vertices, m, _p(src), _p(dst), _p(w), _p(R),
+                                       _p(C), _p(E)))
+    return R, C, E

@@ -1,0 +1,85 @@
+// engine.cuh -- engine and device-graph objects behind the C ABI.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <map>
+#include <utility>
+#include <vector>
+
+#include "common.cuh"
+
+struct kites_engine {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaEvent_t kev0 = nullptr, kev1 = nullptr;   // per-kernel timing
+  cudaMemPool_t pool = nullptr;   // stream-ordered pool owning every buffer
+  int sm_count = 0;
+  int l2_bytes = 0;
+  void *pinned = nullptr;         // small pinned scratch for flag read-backs
+};
+
+namespace kites_internal {
+
+struct loop_key {
+  int op;
+  int strategy;
+  bool operator<(const loop_key &o) const {
+    return op != o.op ? op < o.op : strategy < o.strategy;
+  }
+};
+
+}  // namespace kites_internal
+
+struct kites_graph {
+  kites_engine *eng = nullptr;
+  uint64_t n = 0;          // padded vertex count (multiple of 128)
+  uint64_t n_given = 0;    // rows in the uploaded CSC
+  uint64_t m = 0;
+  uint32_t vpg = 1, shift = 0;
+  int directed = 1;
+  bool off64 = false;      // row arrays are uint64
+  uint32_t vsize = 4, esize = 4;
+
+  void *R = nullptr;       // OffT[n+1]
+  uint32_t *C = nullptr;   // [m]
+  void *E = nullptr;       // [m] x esize
+  void *V = nullptr;       // [n] x vsize
+
+  // Vertex-level out-CSR with weights (rows = sources), built on device.
+  void *outR = nullptr;
+  uint32_t *outC = nullptr;
+  uint32_t *outE = nullptr;
+  uint32_t *out_deg = nullptr;   // [n] out-degree per vertex
+
+  // Activation adjacency (dir_R / dir_C; rows = vertices or groups).
+  void *dirR = nullptr;
+  uint32_t *dirC = nullptr;
+  uint64_t n_dir_rows = 0, n_dir_edges = 0;
+
+  // Edge-balanced chunk tables.
+  uint32_t chunk_items = 2048;
+  uint32_t *chunk_in = nullptr;
+  uint64_t nchunks_in = 0;
+  uint32_t *chunk_dir = nullptr;
+  uint64_t nchunks_dir = 0;
+
+  // Frontier: [f0 | c0 | f1 | c1], nwords each.
+  uint32_t *bitmaps = nullptr;
+  uint64_t nbits = 0, nwords = 0;
+  uint32_t *frontier[2] = {nullptr, nullptr};
+  uint32_t *changed[2] = {nullptr, nullptr};
+
+  kites_internal::run_counters *ctr = nullptr;
+  unsigned long long *rec_active = nullptr;
+  unsigned long long *rec_edges = nullptr;
+
+  // PageRank scratch (allocated on first use).
+  float *pr_x = nullptr, *pr_y = nullptr, *pr_inv_out = nullptr;
+
+  // Instantiated device loops (conditional while graphs), per op/strategy.
+  std::map<kites_internal::loop_key, std::pair<cudaGraph_t, cudaGraphExec_t>> loops;
+
+  std::vector<void *> owned;   // every pool allocation of this graph
+  int pull_grid = 0, expand_grid = 0;
+};

@@ -1,0 +1,426 @@
+// kernels.cuh -- sm_100a kernels of the built-in vertex programs.
+//
+// Layout.  The CSC (rows = destinations, kites/graph/graph_csr.h:28-39) is
+// split once, at upload, into equal chunks of the merged sequence
+// "vertex v, then its in-edges" (item position of v is v + R[v], of edge e
+// of v is v + 1 + e).  A warp owns one chunk at a time, so every warp does
+// the same number of items whatever the degree skew; a hub's row simply
+// spans several chunks and its partial minima meet through atomicMin.
+//
+// Iteration (the reference's pull kernel, kernels_single_device.cuh:18-426,
+// re-designed):
+//   k_pull_chunked    active vertices (bit of the read frontier) reduce
+//                     nbrComp(V[C[e]], E[e]) over their in-edges with a
+//                     warp-segmented min (__reduce_min_sync over runs of
+//                     equal owner), update V in place and mark the
+//                     vertex/group in the `changed` bitmap;
+//   k_expand_chunked  for each changed row of the activation adjacency
+//                     (dir_R/dir_C, or C for undirected graphs) set the
+//                     out-neighbour bits of the write frontier;
+//   memset            clears the read frontier and the changed bitmap
+//                     (compute.cuh:121);
+//   k_loop_check      counts the iteration and ends the loop when no vertex
+//                     changed (compute.cuh:122-128), on the device.
+#pragma once
+#include "common.cuh"
+
+namespace kites_internal {
+
+// ---- chunk table ------------------------------------------------------------
+
+// chunk_v0[k] = largest row r with r + R[r] <= k * chunk_items (k <= nchunks).
+template <typename OffT>
+__global__ void k_chunk_table(const OffT *__restrict__ R, uint64_t n_rows,
+                              uint64_t nchunks, uint32_t chunk_items,
+                              uint32_t *__restrict__ chunk_v0) {
+  uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k > nchunks) return;
+  const uint64_t target = k * chunk_items;
+  uint64_t lo = 0, hi = n_rows;  // answer in [0, n_rows)
+  while (hi - lo > 1) {
+    uint64_t mid = (lo + hi) >> 1;
+    if (mid + (uint64_t)R[mid] <= target) lo = mid; else hi = mid;
+  }
+  chunk_v0[k] = (uint32_t)lo;
+}
+
+template <typename OffT>
+struct chunk_geom {
+  const OffT *R;
+  const uint32_t *C;
+  const uint32_t *chunk_v0;
+  uint64_t nchunks;
+  uint64_t n_rows;
+  uint64_t n_items;
+  uint32_t chunk_items;
+};
+
+// ---- pull -------------------------------------------------------------------
+
+template <typename OffT>
+struct pull_args {
+  chunk_geom<OffT> g;
+  const uint32_t *E;
+  uint32_t *V;
+  const uint32_t *rd;      // read frontier (bit per vertex or per group)
+  uint32_t *chg;           // changed rows of the activation adjacency
+  uint32_t shift;          // log2(vertex_per_group)
+  run_counters *ctr;
+};
+
+template <int OP, typename OffT>
+__global__ void __launch_bounds__(kBlock)
+    k_pull_chunked(pull_args<OffT> a) {
+  if (a.ctr->done) return;
+  __shared__ uint32_t s_ex[kWarpsPerBlock][32];
+  __shared__ OffT s_lo[kWarpsPerBlock][32];
+  __shared__ uint32_t s_acc[kWarpsPerBlock][32];
+  const uint32_t lane = lane_id(), wib = threadIdx.x >> 5;
+  uint32_t *ex = s_ex[wib];
+  OffT *lo_s = s_lo[wib];
+  uint32_t *acc_s = s_acc[wib];
+  unsigned long long n_act = 0, n_edges = 0;
+  const uint64_t stride = (uint64_t)gridDim.x * kWarpsPerBlock;
+  for (uint64_t ch = (uint64_t)blockIdx.x * kWarpsPerBlock + wib;
+       ch < a.g.nchunks; ch += stride) {
+    const int64_t item_lo = (int64_t)(ch * a.g.chunk_items);
+    const int64_t item_hi =
+        min(item_lo + (int64_t)a.g.chunk_items, (int64_t)a.g.n_items);
+    const uint64_t v_first = a.g.chunk_v0[ch];
+    uint64_t v_last = a.g.chunk_v0[ch + 1];
+    if (v_last >= a.g.n_rows) v_last = a.g.n_rows - 1;
+    for (uint64_t vb = v_first & ~31ull; vb <= v_last; vb += 32) {
+      const uint64_t v = vb + lane;
+      const uint32_t word = a.rd[(vb >> a.shift) >> 5];
+      const bool in_range = v >= v_first && v <= v_last;
+      const bool active =
+          in_range && ((word >> ((v >> a.shift) & 31u)) & 1u);
+      if (__ballot_sync(kFull, active) == 0) continue;
+      uint32_t cnt = 0, old = 0;
+      OffT elo = 0;
+      bool whole = false;
+      if (active) {
+        const int64_t r0 = (int64_t)a.g.R[v], r1 = (int64_t)a.g.R[v + 1];
+        const int64_t lo = max(r0, item_lo - (int64_t)v - 1);
+        const int64_t hi = min(r1, item_hi - (int64_t)v - 1);
+        cnt = hi > lo ? (uint32_t)(hi - lo) : 0u;
+        elo = (OffT)lo;
+        whole = (lo == r0) && (hi == r1);
+        const int64_t vpos = (int64_t)v + r0;
+        n_act += (vpos >= item_lo && vpos < item_hi) ? 1 : 0;
+        n_edges += cnt;
+        if (cnt) old = a.V[v];
+      }
+      const uint32_t incl = warp_inclusive_scan(cnt);
+      const uint32_t total = __shfl_sync(kFull, incl, 31);
+      if (total == 0) continue;
+      ex[lane] = incl - cnt;
+      lo_s[lane] = elo;
+      acc_s[lane] = kInf;
+      __syncwarp();
+      for (uint32_t base = 0; base < total; base += 32) {
+        const uint32_t i = base + lane;
+        uint32_t owner = 32u, p = kInf;
+        if (i < total) {
+          uint32_t j = 0;
+#pragma unroll
+          for (uint32_t step = 16; step; step >>= 1)
+            if (ex[j + step] <= i) j += step;
+          owner = j;
+          const OffT e = lo_s[j] + (OffT)(i - ex[j]);
+          const uint32_t src = __ldcs(a.g.C + e);
+          const uint32_t w = op_reads_weights<OP>() ? __ldcs(a.E + e) : 0u;
+          p = nbr_comp<OP>(a.V[src], w);
+        }
+        bool head;
+        const uint32_t rm = run_mask(owner, &head);
+        p = __reduce_min_sync(rm, p);
+        if (head && owner < 32u) acc_s[owner] = min(acc_s[owner], p);
+        __syncwarp();
+      }
+      bool upd = false;
+      if (cnt) {
+        const uint32_t acc = acc_s[lane];
+        if (acc < old) {
+          if (whole) {
+            a.V[v] = acc;
+            upd = true;
+          } else {
+            upd = acc < atomicMin(a.V + v, acc);
+          }
+        }
+      }
+      __syncwarp();
+      const uint32_t gbit = upd ? (1u << ((v >> a.shift) & 31u)) : 0u;
+      const uint32_t bits = __reduce_or_sync(kFull, gbit);
+      if (bits && lane == 0) {
+        atomicOr(a.chg + ((vb >> a.shift) >> 5), bits);
+        a.ctr->update_flag = 1u;
+      }
+    }
+  }
+  n_act = __reduce_add_sync(kFull, (uint32_t)n_act);
+  n_edges = __reduce_add_sync(kFull, (uint32_t)n_edges);
+  if (lane == 0) {
+    if (n_act) atomicAdd(&a.ctr->active, n_act);
+    if (n_edges) atomicAdd(&a.ctr->edges, n_edges);
+  }
+}
+
+// ---- activation -------------------------------------------------------------
+
+template <typename OffT>
+struct expand_args {
+  chunk_geom<OffT> g;      // rows of the activation adjacency
+  const uint32_t *chg;     // changed rows
+  uint32_t *wr;            // write frontier
+  run_counters *ctr;
+};
+
+template <typename OffT>
+__global__ void __launch_bounds__(kBlock)
+    k_expand_chunked(expand_args<OffT> a) {
+  if (a.ctr->done) return;
+  __shared__ uint32_t s_ex[kWarpsPerBlock][32];
+  __shared__ OffT s_lo[kWarpsPerBlock][32];
+  const uint32_t lane = lane_id(), wib = threadIdx.x >> 5;
+  uint32_t *ex = s_ex[wib];
+  OffT *lo_s = s_lo[wib];
+  unsigned long long n_rows = 0, n_edges = 0;
+  const uint64_t stride = (uint64_t)gridDim.x * kWarpsPerBlock;
+  for (uint64_t ch = (uint64_t)blockIdx.x * kWarpsPerBlock + wib;
+       ch < a.g.nchunks; ch += stride) {
+    const int64_t item_lo = (int64_t)(ch * a.g.chunk_items);
+    const int64_t item_hi =
+        min(item_lo + (int64_t)a.g.chunk_items, (int64_t)a.g.n_items);
+    const uint64_t r_first = a.g.chunk_v0[ch];
+    uint64_t r_last = a.g.chunk_v0[ch + 1];
+    if (r_last >= a.g.n_rows) r_last = a.g.n_rows - 1;
+    for (uint64_t rb = r_first & ~31ull; rb <= r_last; rb += 32) {
+      const uint32_t word = a.chg[rb >> 5];
+      if (word == 0) continue;
+      const uint64_t r = rb + lane;
+      const bool active =
+          r >= r_first && r <= r_last && ((word >> lane) & 1u);
+      uint32_t cnt = 0;
+      OffT elo = 0;
+      if (active) {
+        const int64_t r0 = (int64_t)a.g.R[r], r1 = (int64_t)a.g.R[r + 1];
+        const int64_t lo = max(r0, item_lo - (int64_t)r - 1);
+        const int64_t hi = min(r1, item_hi - (int64_t)r - 1);
+        cnt = hi > lo ? (uint32_t)(hi - lo) : 0u;
+        elo = (OffT)lo;
+        const int64_t rpos = (int64_t)r + r0;
+        n_rows += (rpos >= item_lo && rpos < item_hi) ? 1 : 0;
+        n_edges += cnt;
+      }
+      const uint32_t incl = warp_inclusive_scan(cnt);
+      const uint32_t total = __shfl_sync(kFull, incl, 31);
+      if (total == 0) continue;
+      ex[lane] = incl - cnt;
+      lo_s[lane] = elo;
+      __syncwarp();
+      for (uint32_t base = 0; base < total; base += 32) {
+        const uint32_t i = base + lane;
+        uint32_t tword = kFull, tbit = 0;
+        if (i < total) {
+          uint32_t j = 0;
+#pragma unroll
+          for (uint32_t step = 16; step; step >>= 1)
+            if (ex[j + step] <= i) j += step;
+          const OffT e = lo_s[j] + (OffT)(i - ex[j]);
+          const uint32_t t = __ldcs(a.g.C + e);
+          tword = t >> 5;
+          tbit = 1u << (t & 31u);
+        }
+        bool head;
+        const uint32_t rm = run_mask(tword, &head);
+        const uint32_t bits = __reduce_or_sync(rm, tbit);
+        if (head && tword != kFull) atomicOr(a.wr + tword, bits);
+      }
+      __syncwarp();
+    }
+  }
+  n_rows = __reduce_add_sync(kFull, (uint32_t)n_rows);
+  n_edges = __reduce_add_sync(kFull, (uint32_t)n_edges);
+  if (lane == 0) {
+    if (n_rows) atomicAdd(&a.ctr->updated, n_rows);
+    if (n_edges) atomicAdd(&a.ctr->out_edges, n_edges);
+  }
+}
+
+// ---- loop control -----------------------------------------------------------
+
+// Per-iteration bookkeeping, one thread.  With a conditional-node handle it
+// also ends the captured while loop (device-side convergence).
+struct iter_record {
+  unsigned long long *active;
+  unsigned long long *edges;
+  uint32_t capacity;
+};
+
+__global__ void k_loop_check(run_counters *c, iter_record rec,
+                             cudaGraphConditionalHandle handle, int has_handle) {
+  if (c->done) {
+    if (has_handle) cudaGraphSetConditional(handle, 0);
+    return;
+  }
+  const unsigned long long it = c->iterations;
+  if (it < rec.capacity) {
+    if (rec.active) rec.active[it] = c->active;
+    if (rec.edges) rec.edges[it] = c->edges;
+  }
+  c->iterations = it + 1;
+  c->total_active += c->active;
+  c->total_edges += c->edges;
+  c->total_updated += c->updated;
+  c->total_out_edges += c->out_edges;
+  c->active = c->edges = c->updated = c->out_edges = 0;
+  bool stop = false;
+  if (c->update_flag == 0) {
+    stop = true;
+  } else {
+    c->update_flag = 0;
+    if (c->max_iterations && c->iterations >= c->max_iterations) {
+      c->timed_out = 1;
+      stop = true;
+    }
+  }
+  if (stop) {
+    c->done = 1;
+    if (has_handle) cudaGraphSetConditional(handle, 0);
+  }
+}
+
+// ---- initialisation ---------------------------------------------------------
+
+__global__ void k_fill_u32(uint32_t *p, uint64_t n, uint32_t value) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    p[i] = value;
+}
+
+__global__ void k_iota_u32(uint32_t *p, uint64_t n) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    p[i] = (uint32_t)i;
+}
+
+// Sets V[source] = 0 and the frontier bit of every out-neighbour group of
+// `source` (the example's pre-processing: bit d/vpg for each edge source->d).
+template <typename OffT>
+__global__ void k_seed_source(uint32_t *V, const OffT *__restrict__ outR,
+                              const uint32_t *__restrict__ outC, uint32_t source,
+                              uint32_t shift, uint32_t *frontier) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) V[source] = 0u;
+  const OffT b = outR[source], e = outR[source + 1];
+  for (OffT i = b + (OffT)(blockIdx.x * blockDim.x + threadIdx.x); i < e;
+       i += (OffT)(gridDim.x * blockDim.x)) {
+    const uint32_t g = outC[i] >> shift;
+    atomicOr(frontier + (g >> 5), 1u << (g & 31u));
+  }
+}
+
+// Every bit in [0, nbits) set, the rest of the words 0.
+__global__ void k_all_active(uint32_t *bits, uint64_t nbits, uint64_t nwords) {
+  for (uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; w < nwords;
+       w += (uint64_t)gridDim.x * blockDim.x) {
+    uint64_t lo = w * 32;
+    uint32_t m = 0;
+    if (lo + 32 <= nbits) m = kFull;
+    else if (lo < nbits) m = (1u << (uint32_t)(nbits - lo)) - 1u;
+    bits[w] = m;
+  }
+}
+
+// Upload validation: R[0] == 0, R non-decreasing, R[n_rows] == n_edges, and
+// every id of `ids` below `limit`.  Any violation sets *bad; nothing is
+// traversed before these pass, so a malformed graph is an error status,
+// never an out-of-range access.
+template <typename OffT>
+__global__ void k_validate_rows(const OffT *__restrict__ R, uint64_t n_rows,
+                                uint64_t n_edges, uint32_t *bad) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n_rows;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const OffT a = R[i], b = R[i + 1];
+    if (a > b || (i == 0 && a != 0) || (i + 1 == n_rows && (uint64_t)b != n_edges))
+      atomicOr(bad, 1u);
+  }
+}
+
+__global__ void k_validate_ids(const uint32_t *__restrict__ ids, uint64_t n,
+                               uint64_t limit, uint32_t *bad) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    if (ids[i] >= limit) atomicOr(bad, 2u);
+}
+
+// Zeroes `words` words (read frontier + changed bitmap of one parity).
+__global__ void k_clear_words(uint32_t *p, uint64_t words) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < words;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    p[i] = 0u;
+}
+
+// R[n_src+1 .. n_rows] = R[n_src]: empty rows for the 128-padding vertices.
+template <typename OffT>
+__global__ void pad_offsets(OffT *R, uint64_t n_src, uint64_t n_rows) {
+  const OffT last = R[n_src];
+  for (uint64_t i = n_src + 1 + (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+       i <= n_rows; i += (uint64_t)gridDim.x * blockDim.x)
+    R[i] = last;
+}
+
+// ---- out-CSR transposition helpers -------------------------------------------
+
+template <typename OffT>
+__global__ void k_row_of_edge(const OffT *__restrict__ R, uint64_t n_rows,
+                              uint64_t n_edges, uint32_t *__restrict__ row) {
+  for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n_edges;
+       e += (uint64_t)gridDim.x * blockDim.x) {
+    uint64_t lo = 0, hi = n_rows;  // largest r with R[r] <= e
+    while (hi - lo > 1) {
+      uint64_t mid = (lo + hi) >> 1;
+      if ((uint64_t)R[mid] <= e) lo = mid; else hi = mid;
+    }
+    row[e] = (uint32_t)lo;
+  }
+}
+
+__global__ void k_count_u32(const uint32_t *__restrict__ keys, uint64_t n,
+                            uint32_t *__restrict__ counts) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    atomicAdd(counts + keys[i], 1u);
+}
+
+template <typename OffT>
+__global__ void k_gather_out(const uint32_t *__restrict__ order,
+                             const uint32_t *__restrict__ row_of_edge,
+                             const uint32_t *__restrict__ E, uint64_t n,
+                             uint32_t *__restrict__ outC, uint32_t *__restrict__ outE) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t e = order[i];
+    outC[i] = row_of_edge[e];
+    if (outE) outE[i] = E ? E[e] : 1u;
+  }
+}
+
+template <typename OffT>
+__global__ void k_widen_offsets(const uint32_t *__restrict__ in, uint64_t n,
+                                OffT *__restrict__ out) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    out[i] = (OffT)in[i];
+}
+
+template <typename OffT>
+__global__ void k_narrow_offsets(const uint64_t *__restrict__ in, uint64_t n,
+                                 OffT *__restrict__ out) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    out[i] = (OffT)in[i];
+}
+
+}  // namespace kites_internal
