@@ -166,6 +166,9 @@ int kites_engine_destroy(kites_engine *eng);
 int kites_engine_mem_usage(kites_engine *eng, uint64_t *used, uint64_t *total,
                            uint64_t *pool_reserved);
 int kites_engine_sync(kites_engine *eng);  /* nv_gpu::sync (nv_gpu.cuh:45-48) */
+/* The cudaStream_t every engine call is ordered on; replaces
+ * nv_gpu::getSsEven (nv_gpu.cuh:56-58), the reference's working stream. */
+int kites_engine_stream(kites_engine *eng, void **stream_out);
 
 /* ---- graphs ----------------------------------------------------------- */
 

@@ -9,6 +9,7 @@ from __future__ import annotations
 
 import ctypes
 import os
+import weakref
 from ctypes import (POINTER, Structure, c_char_p, c_double, c_float, c_int,
                     c_int32, c_uint8, c_uint32, c_uint64, c_void_p)
 
@@ -29,7 +30,7 @@ INF = 0xFFFFFFFF
 EXPORTED = [
     "kites_last_error_string", "kites_abi_version", "kites_default_run_opts",
     "kites_engine_create", "kites_engine_destroy", "kites_engine_mem_usage",
-    "kites_engine_sync", "kites_graph_upload", "kites_graph_destroy",
+    "kites_engine_sync", "kites_engine_stream", "kites_graph_upload", "kites_graph_destroy",
     "kites_graph_device_view", "kites_graph_get_values", "kites_graph_set_values",
     "kites_graph_set_frontier", "kites_process", "kites_sssp", "kites_sssp_batch",
     "kites_cc", "kites_pagerank", "kites_gen_rmat", "kites_gen_er", "kites_gen_grid",
@@ -113,6 +114,7 @@ def load(path: str = LIB_PATH):
         "kites_engine_mem_usage": (c_int, [vp, POINTER(c_uint64), POINTER(c_uint64),
                                            POINTER(c_uint64)]),
         "kites_engine_sync": (c_int, [vp]),
+        "kites_engine_stream": (c_int, [vp, POINTER(c_void_p)]),
         "kites_graph_upload": (c_int, [vp, POINTER(CscView), POINTER(c_void_p)]),
         "kites_graph_destroy": (c_int, [vp]),
         "kites_graph_device_view": (c_int, [vp, POINTER(DeviceView)]),
@@ -176,10 +178,15 @@ class Engine:
 
     def __init__(self, device: int = 0):
         self._h = c_void_p()
+        self._graphs = weakref.WeakSet()
         _check(load().kites_engine_create(device, ctypes.byref(self._h)))
         self.device = device
 
     def close(self):
+        # The C engine destroys its graphs with it; close the Python handles
+        # first so none of them is destroyed twice.
+        for g in list(self._graphs):
+            g.close()
         if self._h:
             load().kites_engine_destroy(self._h)
             self._h = c_void_p()
@@ -259,6 +266,7 @@ class Graph:
         self._keep = (R, C, E, V, frontier, dir_R, dir_C)
         self._h = c_void_p()
         _check(load().kites_graph_upload(engine._h, ctypes.byref(v), ctypes.byref(self._h)))
+        engine._graphs.add(self)
         self._keep = None
         self.n_vertices = int(v.n_vertices)
         self.n_edges = int(v.n_edges)
@@ -267,7 +275,8 @@ class Graph:
 
     def close(self):
         if self._h:
-            load().kites_graph_destroy(self._h)
+            if self.engine._h:
+                load().kites_graph_destroy(self._h)
             self._h = c_void_p()
 
     def __del__(self):

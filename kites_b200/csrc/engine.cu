@@ -235,7 +235,9 @@ int upload_typed(kites_graph *g, const kites_csc_view *v) {
     KITES_CUDA_TRY(cudaMemcpyAsync(g->V, v->vertex_values, v->n_vertices * g->vsize,
                                    cudaMemcpyDefault, s));
 
-  if (g->esize == 4 || g->esize == 0) KITES_TRY(build_out_csr<OffT>(g));
+  // Out-CSR structure for every graph; its weights only mean something for
+  // 4-byte edge values (other sizes get 1).
+  KITES_TRY(build_out_csr<OffT>(g));
 
   // Activation adjacency.
   if (!g->directed) {
@@ -611,6 +613,8 @@ extern "C" int kites_engine_destroy(kites_engine *eng) {
   if (!eng) return KITES_OK;
   cudaSetDevice(eng->device);
   if (eng->stream) cudaStreamSynchronize(eng->stream);
+  // Graphs die with their engine; their handles are invalid afterwards.
+  while (!eng->graphs.empty()) kites_graph_destroy(eng->graphs.back());
   if (eng->pinned) cudaFreeHost(eng->pinned);
   if (eng->ev0) cudaEventDestroy(eng->ev0);
   if (eng->ev1) cudaEventDestroy(eng->ev1);
@@ -639,6 +643,13 @@ extern "C" int kites_engine_mem_usage(kites_engine *eng, uint64_t *used,
   return KITES_OK;
 }
 
+extern "C" int kites_engine_stream(kites_engine *eng, void **stream_out) {
+  clear_error();
+  if (!eng || !stream_out) return fail(KITES_ERR_INVALID, "null argument");
+  *stream_out = (void *)eng->stream;
+  return KITES_OK;
+}
+
 extern "C" int kites_engine_sync(kites_engine *eng) {
   clear_error();
   if (!eng) return fail(KITES_ERR_INVALID, "null engine");
@@ -657,6 +668,8 @@ extern "C" int kites_graph_destroy(kites_graph *g) {
   }
   for (void *p : g->owned) cudaFreeAsync(p, g->eng->stream);
   cudaStreamSynchronize(g->eng->stream);
+  auto &live = g->eng->graphs;
+  live.erase(std::remove(live.begin(), live.end(), g), live.end());
   delete g;
   return KITES_OK;
 }
@@ -681,6 +694,7 @@ extern "C" int kites_graph_upload(kites_engine *eng, const kites_csc_view *v,
   KITES_TRY(set_device(eng));
   kites_graph *g = new kites_graph();
   g->eng = eng;
+  eng->graphs.push_back(g);
   g->n_given = v->n_vertices;
   g->n = (v->n_vertices + 127) / 128 * 128;
   g->m = v->n_edges;

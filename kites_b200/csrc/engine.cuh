@@ -17,6 +17,7 @@ struct kites_engine {
   int sm_count = 0;
   int l2_bytes = 0;
   void *pinned = nullptr;         // small pinned scratch for flag read-backs
+  std::vector<struct kites_graph *> graphs;   // live graphs, destroyed with the engine
 };
 
 namespace kites_internal {

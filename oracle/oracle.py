@@ -179,9 +179,13 @@ def build_host_graph(first, second, weights=None, *, form_s_d=True, vpg=1,
         act[(src[fire2] // vpg)] = True
         # graph_raw.h:111-121 -- the reverse edge is pushed right after the
         # forward one, with its own pre-processing call.
+        # That call sees the endpoints swapped, so a rule-derived value is
+        # computed for (dst, src); a value read from the file is the same.
+        w_rev = w if (weights is not None or weight_rule is None) else \
+            weight_rule(dst, src).astype(np.uint32)
         rows_dst = np.concatenate([dst, src])
         rows_src = np.concatenate([src, dst])
-        rows_w = np.concatenate([w, w])
+        rows_w = np.concatenate([w, w_rev])
         order_key = np.concatenate([2 * np.arange(ne_in), 2 * np.arange(ne_in) + 1])
 
     order = np.lexsort((order_key, rows_src, rows_dst))
@@ -222,7 +226,8 @@ def build_host_graph(first, second, weights=None, *, form_s_d=True, vpg=1,
         # graph_csr.h:100-104 copies bits only for groups < rawIVecOutgoing.size()
         flags[n_out_groups:] = False
     else:
-        dir_R = np.zeros(1, dtype=np.uint64)
+        # dir_R / dir_C are never allocated for undirected graphs.
+        dir_R = np.zeros(0, dtype=np.uint64)
         dir_C = np.zeros(0, dtype=np.uint32)
         nbits = ngroups
         # rawIVecOutgoing stays empty for undirected graphs, so no bit is
