@@ -219,6 +219,35 @@ int kites_pagerank(kites_engine *eng, kites_graph *g, uint64_t n_real,
                    float *rank_out, const kites_run_opts *opts,
                    kites_run_stats *stats);
 
+/* ---- learned strategy selector ---------------------------------------
+ * No reference counterpart: the reference always runs its one pull kernel.
+ * A 12 -> 32 -> 32 -> 4 FP32 MLP predicts, from frontier statistics, the
+ * log time ratio of each strategy class (PLAIN, PUSH, PULL_ALL, TPV) to
+ * PLAIN for the next iteration; KITES_STRATEGY_AUTO runs the class with the
+ * lowest prediction when it beats PLAIN by more than opts->selector_margin,
+ * else PLAIN.  An engine starts with neutral weights (always PLAIN). */
+#define KITES_SELECTOR_FEATURES 12
+#define KITES_SELECTOR_CLASSES 4
+#define KITES_SELECTOR_PARAMS 1628
+
+/* Training data: single-source run (or CC when op == KITES_OP_CC) where every
+ * iteration first times each class from the same state (then restores it)
+ * and then advances with PLAIN.  features: capacity x 12, times_ms:
+ * capacity x 4 (PLAIN, PUSH, PULL_ALL, TPV). */
+int kites_selector_record(kites_engine *eng, kites_graph *g, int op, uint32_t source,
+                          float *features, float *times_ms, uint32_t capacity,
+                          uint32_t *n_records);
+/* Full-batch Adam on MSE of log(t_class / t_PLAIN), hand-written CUDA
+ * kernels; loads the result into the engine and copies it to params_out. */
+int kites_selector_train(kites_engine *eng, const float *features, const float *times_ms,
+                         uint32_t n_records, uint32_t epochs, float learning_rate,
+                         uint64_t seed, float *params_out, float *final_loss);
+int kites_selector_load(kites_engine *eng, const float *params, uint32_t n_params);
+int kites_selector_save(kites_engine *eng, float *params, uint32_t n_params);
+/* Threads-per-vertex width of the selector's TPV class for this graph
+ * (KITES_STRATEGY_TPV1/4/8/32). */
+int kites_graph_set_tpv(kites_graph *g, int strategy);
+
 /* ---- synthetic graphs (host, deterministic, OpenMP) ------------------ */
 
 /* Candidate edges come from a counter-based SplitMix64 stream; self-loops,

@@ -34,8 +34,14 @@ EXPORTED = [
     "kites_graph_device_view", "kites_graph_get_values", "kites_graph_set_values",
     "kites_graph_set_frontier", "kites_process", "kites_sssp", "kites_sssp_batch",
     "kites_cc", "kites_pagerank", "kites_gen_rmat", "kites_gen_er", "kites_gen_grid",
-    "kites_csc_from_edges",
+    "kites_csc_from_edges", "kites_selector_record", "kites_selector_train",
+    "kites_selector_load", "kites_selector_save", "kites_graph_set_tpv",
 ]
+SELECTOR_FEATURES, SELECTOR_CLASSES, SELECTOR_PARAMS = 12, 4, 1628
+# Parameter layout of the selector MLP (offsets into the 1628 floats).
+SEL_OFF = {"mean": 0, "std": 12, "W1": 24, "b1": 408, "W2": 440, "b2": 1464, "W3": 1496,
+           "b3": 1624}
+CLASS_STRATEGY = [STRATEGY_PLAIN, STRATEGY_PUSH, STRATEGY_PULL_ALL, None]  # None: graph's TPV
 
 
 class CscView(Structure):
@@ -133,6 +139,12 @@ def load(path: str = LIB_PATH):
         "kites_gen_er": (c_int, [u64, u64, u64, u32, u32, vp, vp, vp]),
         "kites_gen_grid": (c_int, [u32, u64, u32, u32, vp, vp, vp]),
         "kites_csc_from_edges": (c_int, [u64, u64, vp, vp, vp, vp, vp, vp]),
+        "kites_selector_record": (c_int, [vp, vp, c_int, u32, vp, vp, u32, POINTER(c_uint32)]),
+        "kites_selector_train": (c_int, [vp, vp, vp, u32, u32, c_float, u64, vp,
+                                         POINTER(c_float)]),
+        "kites_selector_load": (c_int, [vp, vp, u32]),
+        "kites_selector_save": (c_int, [vp, vp, u32]),
+        "kites_graph_set_tpv": (c_int, [vp, c_int]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)
@@ -211,6 +223,25 @@ class Engine:
 
     def sync(self):
         _check(load().kites_engine_sync(self._h))
+
+    # ---- learned selector ----
+    def selector_train(self, features, times_ms, epochs=2000, lr=3e-3, seed=1):
+        X = np.ascontiguousarray(features, dtype=np.float32)
+        T = np.ascontiguousarray(times_ms, dtype=np.float32)
+        params = np.empty(SELECTOR_PARAMS, dtype=np.float32)
+        loss = c_float()
+        _check(load().kites_selector_train(self._h, _p(X), _p(T), X.shape[0], epochs, lr,
+                                           seed, _p(params), ctypes.byref(loss)))
+        return params, loss.value
+
+    def selector_load(self, params):
+        P = np.ascontiguousarray(params, dtype=np.float32)
+        _check(load().kites_selector_load(self._h, _p(P), P.shape[0]))
+
+    def selector_save(self):
+        P = np.empty(SELECTOR_PARAMS, dtype=np.float32)
+        _check(load().kites_selector_save(self._h, _p(P), SELECTOR_PARAMS))
+        return P
 
 
 class Graph:
@@ -334,6 +365,18 @@ class Graph:
         _check(load().kites_sssp_batch(self.engine._h, self._h, op, _p(src), k, _p(out),
                                        ctypes.byref(o), ctypes.byref(st)))
         return out, st
+
+    def selector_record(self, op=OP_SSSP, source=0, capacity=512):
+        """Per iteration: 12 features and the time (ms) of each selector class."""
+        X = np.zeros((capacity, SELECTOR_FEATURES), dtype=np.float32)
+        T = np.zeros((capacity, SELECTOR_CLASSES), dtype=np.float32)
+        n = c_uint32()
+        _check(load().kites_selector_record(self.engine._h, self._h, op, source, _p(X), _p(T),
+                                            capacity, ctypes.byref(n)))
+        return X[: n.value], T[: n.value]
+
+    def set_tpv(self, strategy):
+        _check(load().kites_graph_set_tpv(self._h, strategy))
 
     def cc(self, out=None, opts=None):
         st = RunStats()

@@ -53,6 +53,10 @@ struct run_counters {
   unsigned long long total_updated;
   unsigned long long total_out_edges;
   unsigned long long queue_len[2];    // compacted changed queue lengths
+  unsigned long long last_active;     // active / edges of the previous iteration
+  unsigned long long last_edges;
+  uint32_t sel;                       // strategy class picked for the next iteration
+  uint32_t pad1;
 };
 
 // ---- warp primitives ---------------------------------------------------

@@ -13,7 +13,10 @@
 
 #include "engine.cuh"
 #include "kernels.cuh"
+#include "kernels_batch.cuh"
 #include "kernels_pr.cuh"
+#include "kernels_select.cuh"
+#include "kernels_strategy.cuh"
 
 using namespace kites_internal;
 
@@ -296,14 +299,10 @@ int upload_typed(kites_graph *g, const kites_csc_view *v) {
 
 // ---- iteration loops ----------------------------------------------------
 
-struct loop_ctx {
-  kites_graph *g;
-  int op;
-};
-
+// One iteration of the plain strategy: pull, activation, clear, check.
 template <int OP, typename OffT>
 int launch_iteration(kites_graph *g, int parity, cudaGraphConditionalHandle h,
-                     int has_handle, uint64_t *launches, bool time_pull = false) {
+                     int has_handle, uint64_t *launches, bool time_pull) {
   cudaStream_t s = g->eng->stream;
   if (time_pull) KITES_CUDA_TRY(cudaEventRecord(g->eng->kev0, s));
   chunk_geom<OffT> gin{(const OffT *)g->R, g->C, g->chunk_in, g->nchunks_in,
@@ -326,55 +325,56 @@ int launch_iteration(kites_graph *g, int parity, cudaGraphConditionalHandle h,
   return KITES_OK;
 }
 
-template <int OP, typename OffT>
-int get_device_loop(kites_graph *g, int strategy, cudaGraphExec_t *exec) {
-  loop_key key{OP, strategy};
-  auto it = g->loops.find(key);
-  if (it != g->loops.end()) {
-    *exec = it->second.second;
-    return KITES_OK;
-  }
+// Batched iteration: K-wide pull over the V x K array, vertex-level
+// activation, clear, check.  bits = [f0 | c0 | f1 | c1], nwords each.
+struct batch_state {
+  uint32_t *D;
+  uint32_t *bits;
+  uint64_t nwords;
+  const void *actR;
+  const uint32_t *actC;
+  const uint32_t *act_chunks;
+  uint64_t act_nchunks, act_rows, act_edges;
+  int grid;
+};
+
+template <int OP, typename OffT, int K>
+int launch_batch_iteration(kites_graph *g, const batch_state &b, int parity,
+                           cudaGraphConditionalHandle h, int has_handle, uint64_t *launches,
+                           bool time_pull) {
   cudaStream_t s = g->eng->stream;
-  cudaGraph_t graph;
-  KITES_CUDA_TRY(cudaGraphCreate(&graph, 0));
-  cudaGraphConditionalHandle handle;
-  KITES_CUDA_TRY(cudaGraphConditionalHandleCreate(&handle, graph, 1,
-                                                  cudaGraphCondAssignDefault));
-  cudaGraphNodeParams cp = {};
-  cp.type = cudaGraphNodeTypeConditional;
-  cp.conditional.handle = handle;
-  cp.conditional.type = cudaGraphCondTypeWhile;
-  cp.conditional.size = 1;
-  cudaGraphNode_t node;
-  KITES_CUDA_TRY(cudaGraphAddNode(&node, graph, nullptr, 0, &cp));
-  cudaGraph_t body = cp.conditional.phGraph_out[0];
-  KITES_CUDA_TRY(cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0,
-                                               cudaStreamCaptureModeThreadLocal));
-  uint64_t dummy = 0;
-  int st = launch_iteration<OP, OffT>(g, 0, handle, 1, &dummy);
-  if (st == KITES_OK) st = launch_iteration<OP, OffT>(g, 1, handle, 1, &dummy);
-  cudaGraph_t captured;
-  cudaError_t e = cudaStreamEndCapture(s, &captured);
-  if (st != KITES_OK) return st;
-  KITES_CUDA_TRY(e);
-  cudaGraphExec_t ex;
-  KITES_CUDA_TRY(cudaGraphInstantiate(&ex, graph, 0));
-  g->loops[key] = {graph, ex};
-  *exec = ex;
+  uint32_t *rd = b.bits + (parity ? 2 : 0) * b.nwords;
+  uint32_t *chg = rd + b.nwords;
+  uint32_t *wr = b.bits + (parity ? 0 : 2) * b.nwords;
+  if (time_pull) KITES_CUDA_TRY(cudaEventRecord(g->eng->kev0, s));
+  chunk_geom<OffT> gb{(const OffT *)g->R, g->C, g->chunk_batch, g->nchunks_batch,
+                      g->n, g->n + g->m, g->batch_chunk_items};
+  pull_batch_args<OffT> pa{gb, (const uint32_t *)g->E, b.D, rd, chg, g->ctr};
+  k_pull_batch<OP, OffT, K><<<b.grid, kBlock, 0, s>>>(pa);
+  if (time_pull) KITES_CUDA_TRY(cudaEventRecord(g->eng->kev1, s));
+  chunk_geom<OffT> ga{(const OffT *)b.actR, b.actC, b.act_chunks, b.act_nchunks, b.act_rows,
+                      b.act_rows + b.act_edges, g->chunk_items};
+  expand_args<OffT> ea{ga, chg, wr, g->ctr};
+  k_expand_chunked<OffT><<<g->expand_grid, kBlock, 0, s>>>(ea);
+  k_clear_words<<<grid_for(2 * b.nwords, 256, 4096), 256, 0, s>>>(rd, 2 * b.nwords);
+  iter_record rec{g->rec_active, g->rec_edges, KITES_MAX_RECORDED_ITERS};
+  k_loop_check<<<1, 1, 0, s>>>(g->ctr, rec, h, has_handle);
+  KITES_CUDA_TRY(cudaGetLastError());
+  *launches += 4;
   return KITES_OK;
 }
 
-struct pinned_state {
-  uint32_t done;
-  uint32_t timed_out;
-  unsigned long long iterations;
-};
-
-template <int OP, typename OffT>
-int run_plain(kites_graph *g, const kites_run_opts &o, kites_run_stats *st) {
+// Iterates to the fixed point.  `launch(parity, handle, has_handle,
+// &launches, time_pull)` enqueues one iteration.  Device loop: a CUDA graph
+// whose conditional while node runs two iterations per trip and stops when
+// k_loop_check clears the condition; it is captured once per loop key and
+// reused.  Host loop: one counter read-back per iteration, as
+// compute.cuh:57-128 does; with time_kernels it also times each pull.
+template <class Launch>
+int drive_loop(kites_graph *g, const kites_run_opts &o, loop_key key, Launch launch,
+               run_counters *out, float *ms, uint64_t *launches, kites_run_stats *st) {
   kites_engine *eng = g->eng;
   cudaStream_t s = eng->stream;
-  auto t0 = std::chrono::steady_clock::now();
   run_counters init = {};
   // A monotone program reaches its fixed point within n + 1 rounds; the
   // default cap only ends a loop that cannot converge (e.g. a wrapping add
@@ -384,17 +384,46 @@ int run_plain(kites_graph *g, const kites_run_opts &o, kites_run_stats *st) {
   *hctr = init;
   KITES_CUDA_TRY(cudaMemcpyAsync(g->ctr, hctr, sizeof(run_counters),
                                  cudaMemcpyHostToDevice, s));
-  uint64_t launches = 0;
-  KITES_CUDA_TRY(cudaEventRecord(eng->ev0, s));
-  if (o.device_loop && !o.time_kernels) {
-    cudaGraphExec_t ex;
-    KITES_TRY((get_device_loop<OP, OffT>(g, KITES_STRATEGY_PLAIN, &ex)));
-    KITES_CUDA_TRY(cudaGraphLaunch(ex, s));
+  *launches = 0;
+  const bool dev_loop = o.device_loop && !o.time_kernels;
+  if (dev_loop) {
+    auto it = g->loops.find(key);
+    if (it == g->loops.end()) {
+      cudaGraph_t graph;
+      KITES_CUDA_TRY(cudaGraphCreate(&graph, 0));
+      cudaGraphConditionalHandle handle;
+      KITES_CUDA_TRY(cudaGraphConditionalHandleCreate(&handle, graph, 1,
+                                                      cudaGraphCondAssignDefault));
+      cudaGraphNodeParams cp = {};
+      cp.type = cudaGraphNodeTypeConditional;
+      cp.conditional.handle = handle;
+      cp.conditional.type = cudaGraphCondTypeWhile;
+      cp.conditional.size = 1;
+      cudaGraphNode_t node;
+      KITES_CUDA_TRY(cudaGraphAddNode(&node, graph, nullptr, 0, &cp));
+      cudaGraph_t body = cp.conditional.phGraph_out[0];
+      KITES_CUDA_TRY(cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0,
+                                                   cudaStreamCaptureModeThreadLocal));
+      uint64_t dummy = 0;
+      int st2 = launch(0, handle, 1, &dummy, false);
+      if (st2 == KITES_OK) st2 = launch(1, handle, 1, &dummy, false);
+      cudaGraph_t captured;
+      cudaError_t e = cudaStreamEndCapture(s, &captured);
+      if (st2 != KITES_OK) {
+        cudaGraphDestroy(graph);
+        return st2;
+      }
+      KITES_CUDA_TRY(e);
+      cudaGraphExec_t ex;
+      KITES_CUDA_TRY(cudaGraphInstantiate(&ex, graph, 0));
+      it = g->loops.emplace(key, std::make_pair(graph, ex)).first;
+    }
+    KITES_CUDA_TRY(cudaEventRecord(eng->ev0, s));
+    KITES_CUDA_TRY(cudaGraphLaunch(it->second.second, s));
   } else {
-    // Host-driven loop, one flag read-back per iteration (compute.cuh:57-128).
-    for (uint64_t it = 0;; ++it) {
-      KITES_TRY((launch_iteration<OP, OffT>(g, (int)(it & 1), 0, 0, &launches,
-                                            o.time_kernels != 0)));
+    KITES_CUDA_TRY(cudaEventRecord(eng->ev0, s));
+    for (uint64_t i = 0;; ++i) {
+      KITES_TRY(launch((int)(i & 1), 0, 0, launches, o.time_kernels != 0));
       KITES_CUDA_TRY(cudaMemcpyAsync(hctr, g->ctr, sizeof(run_counters),
                                      cudaMemcpyDeviceToHost, s));
       KITES_CUDA_TRY(cudaStreamSynchronize(s));
@@ -411,49 +440,62 @@ int run_plain(kites_graph *g, const kites_run_opts &o, kites_run_stats *st) {
   KITES_CUDA_TRY(cudaMemcpyAsync(hctr, g->ctr, sizeof(run_counters),
                                  cudaMemcpyDeviceToHost, s));
   KITES_CUDA_TRY(cudaStreamSynchronize(s));
+  KITES_CUDA_TRY(cudaEventElapsedTime(ms, eng->ev0, eng->ev1));
+  if (dev_loop) *launches = 4 * hctr->iterations;  // kernels that did work
+  *out = *hctr;
+  return KITES_OK;
+}
+
+int record_iterations(kites_graph *g, const run_counters &c, int strategy,
+                      kites_run_stats *st) {
+  const uint32_t nrec =
+      (uint32_t)std::min<unsigned long long>(c.iterations, KITES_MAX_RECORDED_ITERS);
+  st->n_recorded = nrec;
+  if (nrec) {
+    KITES_CUDA_TRY(cudaMemcpy(st->iter_active, g->rec_active, nrec * 8, cudaMemcpyDeviceToHost));
+    KITES_CUDA_TRY(cudaMemcpy(st->iter_edges, g->rec_edges, nrec * 8, cudaMemcpyDeviceToHost));
+    for (uint32_t i = 0; i < nrec; ++i) st->iter_strategy[i] = (uint8_t)strategy;
+  }
+  return KITES_OK;
+}
+
+template <int OP, typename OffT>
+int run_plain(kites_graph *g, const kites_run_opts &o, kites_run_stats *st) {
+  auto t0 = std::chrono::steady_clock::now();
+  run_counters c;
   float ms = 0.f;
-  KITES_CUDA_TRY(cudaEventElapsedTime(&ms, eng->ev0, eng->ev1));
-  const bool dev_loop = o.device_loop && !o.time_kernels;
-  if (dev_loop) launches = 4 * hctr->iterations;  // kernels that ran
+  uint64_t launches = 0;
+  auto launch = [g](int parity, cudaGraphConditionalHandle h, int hh, uint64_t *l, bool tp) {
+    return launch_iteration<OP, OffT>(g, parity, h, hh, l, tp);
+  };
+  KITES_TRY(drive_loop(g, o, loop_key{OP, KITES_STRATEGY_PLAIN}, launch, &c, &ms, &launches, st));
   if (st) {
-    st->iterations = hctr->iterations;
+    st->iterations = c.iterations;
     st->device_ms = ms;
-    st->edges_traversed = hctr->total_edges;
+    st->edges_traversed = c.total_edges;
     const uint64_t e_bytes = op_reads_weights<OP>() ? 4 : 0;
     // Algorithmic bytes (plain pull): per iteration 2 x 4 ceil(nbits/32) for
     // the bitmap read and reset, 12 B per active vertex, (4 + eT + vT) per
     // traversed in-edge, vT + 8 per updated row and 8 per activation edge.
     const uint64_t bitmap = 8ull * ((g->nbits + 31) / 32);
-    st->algorithmic_bytes = hctr->iterations * bitmap + 12ull * hctr->total_active +
-                            (8ull + e_bytes) * hctr->total_edges +
-                            12ull * hctr->total_updated + 8ull * hctr->total_out_edges;
-    st->strategy_hist[KITES_STRATEGY_PLAIN] += hctr->iterations;
+    st->algorithmic_bytes = c.iterations * bitmap + 12ull * c.total_active +
+                            (8ull + e_bytes) * c.total_edges + 12ull * c.total_updated +
+                            8ull * c.total_out_edges;
+    st->strategy_hist[KITES_STRATEGY_PLAIN] += c.iterations;
     if (o.time_kernels)
       // Pull kernel alone: frontier words, 12 B per active vertex (V[v],
       // R[v], R[v+1]), (4 C + eT + 4 V[src]) per in-edge, 4 B per store.
-      st->pull_kernel_bytes = hctr->iterations * 4ull * ((g->nbits + 31) / 32) +
-                              12ull * hctr->total_active +
-                              (8ull + e_bytes) * hctr->total_edges +
-                              4ull * hctr->total_updated;
+      st->pull_kernel_bytes = c.iterations * 4ull * ((g->nbits + 31) / 32) +
+                              12ull * c.total_active + (8ull + e_bytes) * c.total_edges +
+                              4ull * c.total_updated;
     st->kernel_launches += launches;
-    if (o.record_iterations) {
-      uint32_t nrec = (uint32_t)std::min<unsigned long long>(hctr->iterations,
-                                                             KITES_MAX_RECORDED_ITERS);
-      st->n_recorded = nrec;
-      if (nrec) {
-        KITES_CUDA_TRY(cudaMemcpy(st->iter_active, g->rec_active, nrec * 8,
-                                  cudaMemcpyDeviceToHost));
-        KITES_CUDA_TRY(cudaMemcpy(st->iter_edges, g->rec_edges, nrec * 8,
-                                  cudaMemcpyDeviceToHost));
-        for (uint32_t i = 0; i < nrec; ++i) st->iter_strategy[i] = KITES_STRATEGY_PLAIN;
-      }
-    }
+    if (o.record_iterations) KITES_TRY(record_iterations(g, c, KITES_STRATEGY_PLAIN, st));
   }
-  if (hctr->timed_out)
+  if (c.timed_out)
     return fail(KITES_ERR_TIMEOUT, "no fixed point after %llu iterations",
-                (unsigned long long)hctr->iterations);
-  auto t1 = std::chrono::steady_clock::now();
-  if (st) st->host_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+                (unsigned long long)c.iterations);
+  if (st)
+    st->host_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   return KITES_OK;
 }
 
@@ -515,6 +557,621 @@ int run_pagerank(kites_graph *g, uint64_t n_real, float *out, const kites_run_op
                       std::chrono::steady_clock::now() - t0).count();
   }
   return KITES_OK;
+}
+
+// ---- flexible loop: one strategy per iteration -------------------------------
+
+// A: frontier scratch; U[parity]: changed by the previous iteration,
+// U[parity ^ 1]: changed by this one; Q: compacted queue for PUSH.
+struct flex_state {
+  uint32_t *A;
+  uint32_t *U[2];
+  uint32_t *Q;
+};
+
+int prepare_flex(kites_graph *g, flex_state *f) {
+  if (g->vpg != 1 || !g->directed)
+    return fail(KITES_ERR_UNSUPPORTED,
+                "per-iteration strategies need a directed graph with vertex_per_group 1");
+  if (!g->queue) {
+    void *p;
+    KITES_TRY(graph_alloc(g, &p, g->n * 4));
+    g->queue = (uint32_t *)p;
+  }
+  f->A = g->frontier[0];
+  f->U[0] = g->changed[0];
+  f->U[1] = g->changed[1];
+  f->Q = g->queue;
+  return KITES_OK;
+}
+
+// Enqueues the kernels of `strategy` for one iteration: U[parity] -> U[parity^1].
+template <int OP, typename OffT>
+int launch_strategy(kites_graph *g, const flex_state &f, int strategy, int parity,
+                    uint64_t *launches) {
+  cudaStream_t s = g->eng->stream;
+  uint32_t *Ucur = f.U[parity], *Unext = f.U[parity ^ 1];
+  chunk_geom<OffT> gin{(const OffT *)g->R, g->C, g->chunk_in, g->nchunks_in,
+                       g->n, g->n + g->m, g->chunk_items};
+  chunk_geom<OffT> gdir{(const OffT *)g->dirR, g->dirC, g->chunk_dir, g->nchunks_dir,
+                        g->n_dir_rows, g->n_dir_rows + g->n_dir_edges, g->chunk_items};
+  const uint64_t nw = g->nwords;
+  auto expand = [&]() {
+    expand_args<OffT> ea{gdir, Ucur, f.A, g->ctr};
+    k_expand_chunked<OffT><<<g->expand_grid, kBlock, 0, s>>>(ea);
+    ++*launches;
+  };
+  switch (strategy) {
+    case KITES_STRATEGY_PLAIN: {
+      expand();
+      pull_args<OffT> pa{gin, (const uint32_t *)g->E, (uint32_t *)g->V, f.A, Unext, 0, g->ctr};
+      k_pull_chunked<OP, OffT><<<g->pull_grid, kBlock, 0, s>>>(pa);
+      break;
+    }
+    case KITES_STRATEGY_PUSH: {
+      k_compact_queue<<<grid_for(nw, 256, 2048), 256, 0, s>>>(Ucur, nw, g->out_deg, f.Q, g->ctr);
+      push_args<OffT> pa{(const OffT *)g->outR, g->outC, g->outE, f.Q, (uint32_t *)g->V, Unext,
+                         g->ctr};
+      k_push_queue<OP, OffT><<<g->eng->sm_count * 8, kBlock, 0, s>>>(pa);
+      ++*launches;
+      break;
+    }
+    case KITES_STRATEGY_PULL_ALL: {
+      pull_args<OffT> pa{gin, (const uint32_t *)g->E, (uint32_t *)g->V, nullptr, Unext, 0,
+                         g->ctr, Ucur};
+      k_pull_all<OP, OffT><<<g->pull_grid, kBlock, 0, s>>>(pa);
+      break;
+    }
+    case KITES_STRATEGY_TPV1:
+    case KITES_STRATEGY_TPV4:
+    case KITES_STRATEGY_TPV8:
+    case KITES_STRATEGY_TPV32: {
+      expand();
+      pull_tpv_args<OffT> pa{(const OffT *)g->R, g->C, (const uint32_t *)g->E,
+                             (uint32_t *)g->V, f.A, Unext, nw, g->ctr};
+      const unsigned grid = grid_for(nw * 32, kBlock, g->eng->sm_count * 16);
+      if (strategy == KITES_STRATEGY_TPV1)
+        k_pull_tpv<OP, OffT, 1><<<grid, kBlock, 0, s>>>(pa);
+      else if (strategy == KITES_STRATEGY_TPV4)
+        k_pull_tpv<OP, OffT, 4><<<grid, kBlock, 0, s>>>(pa);
+      else if (strategy == KITES_STRATEGY_TPV8)
+        k_pull_tpv<OP, OffT, 8><<<grid, kBlock, 0, s>>>(pa);
+      else
+        k_pull_tpv<OP, OffT, 32><<<grid, kBlock, 0, s>>>(pa);
+      break;
+    }
+    default:
+      return fail(KITES_ERR_INVALID, "unknown strategy %d", strategy);
+  }
+  ++*launches;
+  KITES_CUDA_TRY(cudaGetLastError());
+  return KITES_OK;
+}
+
+template <int OP, typename OffT>
+int launch_flex_iteration(kites_graph *g, const flex_state &f, int strategy, int parity,
+                          cudaGraphConditionalHandle h, int hh, uint64_t *launches,
+                          bool time_pull) {
+  cudaStream_t s = g->eng->stream;
+  if (time_pull) KITES_CUDA_TRY(cudaEventRecord(g->eng->kev0, s));
+  KITES_TRY((launch_strategy<OP, OffT>(g, f, strategy, parity, launches)));
+  if (time_pull) KITES_CUDA_TRY(cudaEventRecord(g->eng->kev1, s));
+  k_clear_two<<<grid_for(g->nwords, 256, 4096), 256, 0, s>>>(f.A, f.U[parity], g->nwords);
+  iter_record rec{g->rec_active, g->rec_edges, KITES_MAX_RECORDED_ITERS};
+  k_loop_check<<<1, 1, 0, s>>>(g->ctr, rec, h, hh);
+  KITES_CUDA_TRY(cudaGetLastError());
+  *launches += 2;
+  return KITES_OK;
+}
+
+// Runs the graph's current values from the changed set in U[0] with one
+// fixed strategy per iteration.
+template <int OP, typename OffT>
+int run_flex(kites_graph *g, const kites_run_opts &o, kites_run_stats *st) {
+  auto t0 = std::chrono::steady_clock::now();
+  flex_state f;
+  KITES_TRY(prepare_flex(g, &f));
+  const int strategy = o.strategy;
+  run_counters c;
+  float ms = 0.f;
+  uint64_t launches = 0;
+  auto launch = [g, &f, strategy](int parity, cudaGraphConditionalHandle h, int hh,
+                                  uint64_t *l, bool tp) {
+    return launch_flex_iteration<OP, OffT>(g, f, strategy, parity, h, hh, l, tp);
+  };
+  KITES_TRY(drive_loop(g, o, loop_key{OP, 100 + strategy}, launch, &c, &ms, &launches, st));
+  if (st) {
+    st->iterations = c.iterations;
+    st->device_ms = ms;
+    st->edges_traversed = c.total_edges;
+    const uint64_t e_bytes = op_reads_weights<OP>() ? 4 : 0;
+    st->algorithmic_bytes = c.iterations * 8ull * g->nwords + 12ull * c.total_active +
+                            (8ull + e_bytes) * c.total_edges + 12ull * c.total_updated +
+                            8ull * c.total_out_edges;
+    st->strategy_hist[strategy] += c.iterations;
+    st->kernel_launches += launches;
+    if (o.record_iterations) KITES_TRY(record_iterations(g, c, strategy, st));
+    st->host_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  }
+  if (c.timed_out)
+    return fail(KITES_ERR_TIMEOUT, "no fixed point after %llu iterations",
+                (unsigned long long)c.iterations);
+  return KITES_OK;
+}
+
+template <typename OffT>
+int dispatch_flex(kites_graph *g, int op, const kites_run_opts &o, kites_run_stats *st) {
+  switch (op) {
+    case OP_SSSP: return run_flex<OP_SSSP, OffT>(g, o, st);
+    case OP_SSSP_WRAP: return run_flex<OP_SSSP_WRAP, OffT>(g, o, st);
+    case OP_BFS: return run_flex<OP_BFS, OffT>(g, o, st);
+    case OP_CC: return run_flex<OP_CC, OffT>(g, o, st);
+    default: return fail(KITES_ERR_UNSUPPORTED, "operator %d has no iteration loop", op);
+  }
+}
+
+// ---- learned selection (AUTO) ------------------------------------------------
+
+// Strategy of each selector class.
+int class_strategy(const kites_graph *g, uint32_t cls) {
+  switch (cls) {
+    case 1: return KITES_STRATEGY_PUSH;
+    case 2: return KITES_STRATEGY_PULL_ALL;
+    case 3: return g->tpv_strategy;
+    default: return KITES_STRATEGY_PLAIN;
+  }
+}
+
+int prepare_select(kites_graph *g) {
+  void *p;
+  if (!g->sacc) {
+    KITES_TRY(graph_alloc(g, &p, sizeof(select_acc)));
+    g->sacc = p;
+    KITES_CUDA_TRY(cudaMemsetAsync(p, 0, sizeof(select_acc), g->eng->stream));
+  }
+  if (!g->rec_sel) {
+    KITES_TRY(graph_alloc(g, &p, KITES_MAX_RECORDED_ITERS));
+    g->rec_sel = (uint8_t *)p;
+  }
+  return KITES_OK;
+}
+
+template <typename OffT>
+int launch_select(kites_graph *g, const uint32_t *U, float margin, float *feat_out,
+                  uint32_t feat_cap, cudaGraphConditionalHandle h, int hh, uint64_t *launches) {
+  select_args<OffT> a{U, g->nwords, g->out_deg, (const OffT *)g->R, g->n, g->m, g->ctr,
+                      (select_acc *)g->sacc, g->eng->sel_params, logf(1.f + margin), feat_out,
+                      feat_cap, h, hh};
+  k_select<OffT><<<grid_for(g->nwords, 256, (unsigned)g->eng->sm_count * 4), 256, 0,
+                   g->eng->stream>>>(a);
+  k_record_sel<<<1, 1, 0, g->eng->stream>>>(g->ctr, g->rec_sel, KITES_MAX_RECORDED_ITERS);
+  *launches += 2;
+  KITES_CUDA_TRY(cudaGetLastError());
+  return KITES_OK;
+}
+
+// Captures fn() into `graph` after `deps`; returns the capture's leaf nodes.
+template <class Fn>
+int capture_into(cudaStream_t s, cudaGraph_t graph, const std::vector<cudaGraphNode_t> &deps,
+                 Fn fn, std::vector<cudaGraphNode_t> *leaves) {
+  KITES_CUDA_TRY(cudaStreamBeginCaptureToGraph(s, graph, deps.empty() ? nullptr : deps.data(),
+                                               nullptr, deps.size(),
+                                               cudaStreamCaptureModeThreadLocal));
+  int st = fn();
+  if (leaves && st == KITES_OK) {
+    cudaStreamCaptureStatus cs;
+    const cudaGraphNode_t *d = nullptr;
+    size_t nd = 0;
+    cudaError_t e = cudaStreamGetCaptureInfo(s, &cs, nullptr, nullptr, &d, &nd);
+    if (e == cudaSuccess) leaves->assign(d, d + nd);
+    else st = fail(KITES_ERR_CUDA, "capture info: %s", cudaGetErrorString(e));
+  }
+  cudaGraph_t out;
+  cudaError_t e = cudaStreamEndCapture(s, &out);
+  if (st != KITES_OK) return st;
+  KITES_CUDA_TRY(e);
+  return KITES_OK;
+}
+
+// Device loop of AUTO: while(not converged) { select; switch(class) {PLAIN,
+// PUSH, PULL_ALL, TPV}; clear; check } for both parities.
+template <int OP, typename OffT>
+int build_auto_loop(kites_graph *g, const flex_state &f, float margin, cudaGraphExec_t *exec) {
+  cudaStream_t s = g->eng->stream;
+  cudaGraph_t graph;
+  KITES_CUDA_TRY(cudaGraphCreate(&graph, 0));
+  cudaGraphConditionalHandle hw;
+  KITES_CUDA_TRY(cudaGraphConditionalHandleCreate(&hw, graph, 1, cudaGraphCondAssignDefault));
+  cudaGraphNodeParams wp = {};
+  wp.type = cudaGraphNodeTypeConditional;
+  wp.conditional.handle = hw;
+  wp.conditional.type = cudaGraphCondTypeWhile;
+  wp.conditional.size = 1;
+  cudaGraphNode_t wnode;
+  KITES_CUDA_TRY(cudaGraphAddNode(&wnode, graph, nullptr, 0, &wp));
+  cudaGraph_t body = wp.conditional.phGraph_out[0];
+  std::vector<cudaGraphNode_t> leaves;
+  uint64_t dummy = 0;
+  for (int parity = 0; parity < 2; ++parity) {
+    cudaGraphConditionalHandle hs;
+    KITES_CUDA_TRY(cudaGraphConditionalHandleCreate(&hs, body, 0, cudaGraphCondAssignDefault));
+    std::vector<cudaGraphNode_t> sel_leaves;
+    KITES_TRY(capture_into(s, body, leaves, [&] {
+      return launch_select<OffT>(g, f.U[parity], margin, nullptr, 0, hs, 1, &dummy);
+    }, &sel_leaves));
+    cudaGraphNodeParams sp = {};
+    sp.type = cudaGraphNodeTypeConditional;
+    sp.conditional.handle = hs;
+    sp.conditional.type = cudaGraphCondTypeSwitch;
+    sp.conditional.size = kClasses;
+    cudaGraphNode_t snode;
+    KITES_CUDA_TRY(cudaGraphAddNode(&snode, body, sel_leaves.data(), sel_leaves.size(), &sp));
+    for (int c = 0; c < kClasses; ++c) {
+      cudaGraph_t branch = sp.conditional.phGraph_out[c];
+      const int strat = class_strategy(g, (uint32_t)c);
+      KITES_TRY(capture_into(s, branch, {}, [&] {
+        return launch_strategy<OP, OffT>(g, f, strat, parity, &dummy);
+      }, nullptr));
+    }
+    KITES_TRY(capture_into(s, body, {snode}, [&]() -> int {
+      k_clear_two<<<grid_for(g->nwords, 256, 4096), 256, 0, s>>>(f.A, f.U[parity], g->nwords);
+      iter_record rec{g->rec_active, g->rec_edges, KITES_MAX_RECORDED_ITERS};
+      k_loop_check<<<1, 1, 0, s>>>(g->ctr, rec, hw, 1);
+      KITES_CUDA_TRY(cudaGetLastError());
+      return KITES_OK;
+    }, &leaves));
+  }
+  KITES_CUDA_TRY(cudaGraphInstantiate(exec, graph, 0));
+  g->loops.emplace(loop_key{OP, 200}, std::make_pair(graph, *exec));
+  return KITES_OK;
+}
+
+template <int OP, typename OffT>
+int run_auto(kites_graph *g, const kites_run_opts &o, kites_run_stats *st) {
+  kites_engine *eng = g->eng;
+  cudaStream_t s = eng->stream;
+  auto t0 = std::chrono::steady_clock::now();
+  flex_state f;
+  KITES_TRY(prepare_flex(g, &f));
+  KITES_TRY(prepare_select(g));
+  run_counters init = {};
+  init.max_iterations = o.max_iterations ? o.max_iterations : 2 * g->n + 16;
+  run_counters *hctr = (run_counters *)eng->pinned;
+  *hctr = init;
+  KITES_CUDA_TRY(cudaMemcpyAsync(g->ctr, hctr, sizeof(run_counters), cudaMemcpyHostToDevice, s));
+  uint64_t launches = 0;
+  const bool dev_loop = o.device_loop && !o.time_kernels;
+  if (dev_loop) {
+    // The cached loop bakes in the margin it was captured with.
+    auto it = g->loops.find(loop_key{OP, 200});
+    cudaGraphExec_t ex;
+    if (it != g->loops.end() && g->auto_margin != o.selector_margin) {
+      cudaGraphExecDestroy(it->second.second);
+      cudaGraphDestroy(it->second.first);
+      g->loops.erase(it);
+      it = g->loops.end();
+    }
+    if (it == g->loops.end()) {
+      KITES_TRY((build_auto_loop<OP, OffT>(g, f, o.selector_margin, &ex)));
+      g->auto_margin = o.selector_margin;
+    } else {
+      ex = it->second.second;
+    }
+    KITES_CUDA_TRY(cudaEventRecord(eng->ev0, s));
+    KITES_CUDA_TRY(cudaGraphLaunch(ex, s));
+  } else {
+    KITES_CUDA_TRY(cudaEventRecord(eng->ev0, s));
+    for (uint64_t i = 0;; ++i) {
+      const int parity = (int)(i & 1);
+      KITES_TRY(launch_select<OffT>(g, f.U[parity], o.selector_margin, nullptr, 0, 0, 0,
+                                    &launches));
+      KITES_CUDA_TRY(cudaMemcpyAsync(hctr, g->ctr, sizeof(run_counters), cudaMemcpyDeviceToHost, s));
+      KITES_CUDA_TRY(cudaStreamSynchronize(s));
+      const int strat = class_strategy(g, hctr->sel);
+      KITES_TRY((launch_flex_iteration<OP, OffT>(g, f, strat, parity, 0, 0, &launches,
+                                                 o.time_kernels != 0)));
+      KITES_CUDA_TRY(cudaMemcpyAsync(hctr, g->ctr, sizeof(run_counters), cudaMemcpyDeviceToHost, s));
+      KITES_CUDA_TRY(cudaStreamSynchronize(s));
+      if (o.time_kernels && st) {
+        float kms = 0.f;
+        KITES_CUDA_TRY(cudaEventElapsedTime(&kms, eng->kev0, eng->kev1));
+        st->pull_kernel_ms += kms;
+        st->pull_kernel_launches += 1;
+      }
+      if (hctr->done) break;
+    }
+  }
+  KITES_CUDA_TRY(cudaEventRecord(eng->ev1, s));
+  KITES_CUDA_TRY(cudaMemcpyAsync(hctr, g->ctr, sizeof(run_counters), cudaMemcpyDeviceToHost, s));
+  KITES_CUDA_TRY(cudaStreamSynchronize(s));
+  run_counters c = *hctr;
+  float ms = 0.f;
+  KITES_CUDA_TRY(cudaEventElapsedTime(&ms, eng->ev0, eng->ev1));
+  if (st) {
+    const uint32_t nrec =
+        (uint32_t)std::min<unsigned long long>(c.iterations, KITES_MAX_RECORDED_ITERS);
+    std::vector<uint8_t> cls(nrec);
+    if (nrec)
+      KITES_CUDA_TRY(cudaMemcpy(cls.data(), g->rec_sel, nrec, cudaMemcpyDeviceToHost));
+    for (uint32_t i = 0; i < nrec; ++i) st->strategy_hist[class_strategy(g, cls[i])] += 1;
+    st->iterations = c.iterations;
+    st->device_ms = ms;
+    st->edges_traversed = c.total_edges;
+    const uint64_t e_bytes = op_reads_weights<OP>() ? 4 : 0;
+    st->algorithmic_bytes = c.iterations * 8ull * g->nwords + 12ull * c.total_active +
+                            (8ull + e_bytes) * c.total_edges + 12ull * c.total_updated +
+                            8ull * c.total_out_edges;
+    st->kernel_launches += dev_loop ? 6ull * c.iterations : launches;
+    if (o.record_iterations) {
+      KITES_TRY(record_iterations(g, c, KITES_STRATEGY_AUTO, st));
+      for (uint32_t i = 0; i < nrec && i < st->n_recorded; ++i)
+        st->iter_strategy[i] = (uint8_t)class_strategy(g, cls[i]);
+    }
+    st->host_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  }
+  if (c.timed_out)
+    return fail(KITES_ERR_TIMEOUT, "no fixed point after %llu iterations",
+                (unsigned long long)c.iterations);
+  return KITES_OK;
+}
+
+template <typename OffT>
+int dispatch_auto(kites_graph *g, int op, const kites_run_opts &o, kites_run_stats *st) {
+  switch (op) {
+    case OP_SSSP: return run_auto<OP_SSSP, OffT>(g, o, st);
+    case OP_SSSP_WRAP: return run_auto<OP_SSSP_WRAP, OffT>(g, o, st);
+    case OP_BFS: return run_auto<OP_BFS, OffT>(g, o, st);
+    case OP_CC: return run_auto<OP_CC, OffT>(g, o, st);
+    default: return fail(KITES_ERR_UNSUPPORTED, "operator %d has no iteration loop", op);
+  }
+}
+
+// Training data: from the state at the start of every iteration, run each
+// selector class once (timed with CUDA events) and restore the state; then
+// advance with PLAIN.  Returns per iteration the 12 features and the 4
+// class times in ms.
+template <int OP, typename OffT>
+int record_classes(kites_graph *g, float *feat, float *times, uint32_t cap, uint32_t *n_out) {
+  kites_engine *eng = g->eng;
+  cudaStream_t s = eng->stream;
+  flex_state f;
+  KITES_TRY(prepare_flex(g, &f));
+  KITES_TRY(prepare_select(g));
+  void *p;
+  KITES_TRY(dev_alloc(eng, &p, (uint64_t)cap * kFeat * 4));
+  float *dfeat = (float *)p;
+  KITES_TRY(dev_alloc(eng, &p, g->n * 4 + 2 * g->nwords * 4 + sizeof(run_counters)));
+  uint32_t *snapV = (uint32_t *)p;
+  uint32_t *snapU = snapV + g->n;
+  run_counters *snapC = (run_counters *)(snapU + 2 * g->nwords);
+  run_counters *hctr = (run_counters *)eng->pinned;
+  *hctr = run_counters{};
+  hctr->max_iterations = 2 * g->n + 16;
+  KITES_CUDA_TRY(cudaMemcpyAsync(g->ctr, hctr, sizeof(run_counters), cudaMemcpyHostToDevice, s));
+  uint64_t launches = 0;
+  uint32_t n = 0;
+  int st = KITES_OK;
+  for (uint64_t i = 0; i < cap; ++i) {
+    const int parity = (int)(i & 1);
+    if ((st = launch_select<OffT>(g, f.U[parity], 0.f, dfeat, cap, 0, 0, &launches)) != KITES_OK)
+      break;
+    cudaMemcpyAsync(snapV, g->V, g->n * 4, cudaMemcpyDeviceToDevice, s);
+    cudaMemcpyAsync(snapU, f.U[0], g->nwords * 4, cudaMemcpyDeviceToDevice, s);
+    cudaMemcpyAsync(snapU + g->nwords, f.U[1], g->nwords * 4, cudaMemcpyDeviceToDevice, s);
+    cudaMemcpyAsync(snapC, g->ctr, sizeof(run_counters), cudaMemcpyDeviceToDevice, s);
+    for (uint32_t c = 0; c < (uint32_t)kClasses; ++c) {
+      cudaMemsetAsync(f.A, 0, g->nwords * 4, s);
+      cudaEventRecord(eng->kev0, s);
+      st = launch_strategy<OP, OffT>(g, f, class_strategy(g, c), parity, &launches);
+      cudaEventRecord(eng->kev1, s);
+      if (st != KITES_OK) break;
+      cudaMemcpyAsync(g->V, snapV, g->n * 4, cudaMemcpyDeviceToDevice, s);
+      cudaMemcpyAsync(f.U[0], snapU, g->nwords * 4, cudaMemcpyDeviceToDevice, s);
+      cudaMemcpyAsync(f.U[1], snapU + g->nwords, g->nwords * 4, cudaMemcpyDeviceToDevice, s);
+      cudaMemcpyAsync(g->ctr, snapC, sizeof(run_counters), cudaMemcpyDeviceToDevice, s);
+      cudaError_t e = cudaStreamSynchronize(s);
+      if (e != cudaSuccess) { st = fail(KITES_ERR_CUDA, "record: %s", cudaGetErrorString(e)); break; }
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, eng->kev0, eng->kev1);
+      times[(uint64_t)n * kClasses + c] = ms;
+    }
+    if (st != KITES_OK) break;
+    cudaMemsetAsync(f.A, 0, g->nwords * 4, s);
+    if ((st = launch_flex_iteration<OP, OffT>(g, f, KITES_STRATEGY_PLAIN, parity, 0, 0, &launches,
+                                              false)) != KITES_OK)
+      break;
+    cudaMemcpyAsync(hctr, g->ctr, sizeof(run_counters), cudaMemcpyDeviceToHost, s);
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) { st = fail(KITES_ERR_CUDA, "record: %s", cudaGetErrorString(e)); break; }
+    ++n;
+    if (hctr->done) break;
+  }
+  if (st == KITES_OK && n) {
+    cudaError_t e = cudaMemcpy(feat, dfeat, (uint64_t)n * kFeat * 4, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) st = fail(KITES_ERR_CUDA, "record copy: %s", cudaGetErrorString(e));
+  }
+  cudaFreeAsync(dfeat, s);
+  cudaFreeAsync(snapV, s);
+  cudaStreamSynchronize(s);
+  *n_out = n;
+  return st;
+}
+
+template <typename OffT>
+int dispatch_record(kites_graph *g, int op, float *feat, float *times, uint32_t cap,
+                    uint32_t *n_out) {
+  switch (op) {
+    case OP_SSSP: return record_classes<OP_SSSP, OffT>(g, feat, times, cap, n_out);
+    case OP_BFS: return record_classes<OP_BFS, OffT>(g, feat, times, cap, n_out);
+    case OP_CC: return record_classes<OP_CC, OffT>(g, feat, times, cap, n_out);
+    default: return fail(KITES_ERR_UNSUPPORTED, "recording takes SSSP, BFS or CC");
+  }
+}
+
+// ---- batched multi-source runs -------------------------------------------
+
+void graph_release(kites_graph *g, void *p) {
+  if (!p) return;
+  cudaFreeAsync(p, g->eng->stream);
+  auto &o = g->owned;
+  o.erase(std::remove(o.begin(), o.end(), p), o.end());
+}
+
+void drop_batch_loops(kites_graph *g) {
+  for (auto it = g->loops.begin(); it != g->loops.end();) {
+    if (it->first.strategy >= 1000) {
+      cudaGraphExecDestroy(it->second.second);
+      cudaGraphDestroy(it->second.first);
+      it = g->loops.erase(it);
+    } else {
+      ++it;
+    }
+  }
+}
+
+// Buffers and tables of the batched path for K sources with chunk size
+// `items`; reallocating anything the captured loops point at drops them.
+template <typename OffT>
+int prepare_batch(kites_graph *g, uint32_t K, uint32_t items, batch_state *b) {
+  kites_engine *eng = g->eng;
+  void *p;
+  const uint64_t need = g->n * (uint64_t)K;
+  if (g->batch_cap < need) {
+    drop_batch_loops(g);
+    graph_release(g, g->batchD);
+    KITES_TRY(graph_alloc(g, &p, need * 4));
+    g->batchD = (uint32_t *)p;
+    g->batch_cap = need;
+  }
+  if (!g->d_sources) {
+    KITES_TRY(graph_alloc(g, &p, 256 * 4));
+    g->d_sources = (uint32_t *)p;
+  }
+  if (g->batch_chunk_items != items) {
+    drop_batch_loops(g);
+    graph_release(g, g->chunk_batch);
+    g->batch_chunk_items = items;
+    const uint64_t total = g->n + g->m;
+    uint64_t nc = (total + items - 1) / items;
+    if (nc == 0) nc = 1;
+    KITES_TRY(graph_alloc(g, &p, (nc + 1) * 4));
+    g->chunk_batch = (uint32_t *)p;
+    g->nchunks_batch = nc;
+    k_chunk_table<OffT><<<grid_for(nc + 1), 256, 0, eng->stream>>>(
+        (const OffT *)g->R, g->n, nc, items, g->chunk_batch);
+    KITES_CUDA_TRY(cudaGetLastError());
+  }
+  if (g->vpg == 1) {
+    b->bits = g->bitmaps;
+    b->nwords = g->nwords;
+  } else {
+    if (!g->bbits) {
+      g->bnwords = ((g->n + 31) / 32 + 31) / 32 * 32;
+      KITES_TRY(graph_alloc(g, &p, 4 * g->bnwords * 4));
+      g->bbits = (uint32_t *)p;
+    }
+    b->bits = g->bbits;
+    b->nwords = g->bnwords;
+  }
+  // Vertex-level activation adjacency.
+  if (!g->directed) {
+    b->actR = g->R; b->actC = g->C; b->act_chunks = g->chunk_in;
+    b->act_nchunks = g->nchunks_in; b->act_rows = g->n; b->act_edges = g->m;
+  } else if (g->vpg == 1) {
+    b->actR = g->dirR; b->actC = g->dirC; b->act_chunks = g->chunk_dir;
+    b->act_nchunks = g->nchunks_dir; b->act_rows = g->n; b->act_edges = g->m;
+  } else {
+    if (!g->chunk_out)
+      KITES_TRY(build_chunk_table<OffT>(g, (const OffT *)g->outR, g->n, g->m, &g->chunk_out,
+                                        &g->nchunks_out));
+    b->actR = g->outR; b->actC = g->outC; b->act_chunks = g->chunk_out;
+    b->act_nchunks = g->nchunks_out; b->act_rows = g->n; b->act_edges = g->m;
+  }
+  b->D = g->batchD;
+  return KITES_OK;
+}
+
+template <int OP, typename OffT, int K>
+int run_batch(kites_graph *g, const uint32_t *sources, uint32_t *dist_out,
+              const kites_run_opts &o, kites_run_stats *st) {
+  kites_engine *eng = g->eng;
+  cudaStream_t s = eng->stream;
+  auto t0 = std::chrono::steady_clock::now();
+  batch_state b{};
+  const uint32_t items = g->batch_chunk_items ? g->batch_chunk_items : 256u;
+  KITES_TRY(prepare_batch<OffT>(g, K, items, &b));
+  int per_sm = 0;
+  KITES_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+      &per_sm, k_pull_batch<OP, OffT, K>, kBlock, 0));
+  const uint64_t cap = (uint64_t)std::max(per_sm, 1) * eng->sm_count;
+  const uint64_t want = (g->nchunks_batch + kWarpsPerBlock - 1) / kWarpsPerBlock;
+  b.grid = (int)std::max<uint64_t>(1, std::min(want, cap));
+  KITES_CUDA_TRY(cudaMemcpyAsync(g->d_sources, sources, K * 4, cudaMemcpyDefault, s));
+  k_fill_u32<<<grid_for(g->n * K), 256, 0, s>>>(b.D, g->n * K, kInf);
+  KITES_CUDA_TRY(cudaMemsetAsync(b.bits, 0, 4 * b.nwords * 4, s));
+  k_seed_batch<OffT><<<K, 256, 0, s>>>(b.D, K, g->d_sources, (const OffT *)g->outR, g->outC,
+                                       b.bits);
+  KITES_CUDA_TRY(cudaGetLastError());
+  run_counters c;
+  float ms = 0.f;
+  uint64_t launches = 0;
+  auto launch = [g, &b](int parity, cudaGraphConditionalHandle h, int hh, uint64_t *l, bool tp) {
+    return launch_batch_iteration<OP, OffT, K>(g, b, parity, h, hh, l, tp);
+  };
+  KITES_TRY(drive_loop(g, o, loop_key{OP, 1000 + (int)K}, launch, &c, &ms, &launches, st));
+  if (dist_out) {
+    KITES_CUDA_TRY(cudaMemcpyAsync(dist_out, b.D, g->n_given * K * 4, cudaMemcpyDefault, s));
+    KITES_CUDA_TRY(cudaStreamSynchronize(s));
+  }
+  if (st) {
+    st->iterations = c.iterations;
+    st->device_ms = ms;
+    st->edges_traversed = c.total_edges;
+    const uint64_t e_bytes = op_reads_weights<OP>() ? 4 : 0;
+    // Batched pull: per traversed in-edge C + eT + the K-wide source row;
+    // per active vertex R pair + its K-wide row read (and write if updated).
+    const uint64_t bitmap = 8ull * b.nwords;
+    st->algorithmic_bytes = c.iterations * bitmap + (8ull + 4ull * K) * c.total_active +
+                            (4ull + e_bytes + 4ull * K) * c.total_edges +
+                            (4ull * K + 8ull) * c.total_updated + 8ull * c.total_out_edges;
+    if (o.time_kernels)
+      st->pull_kernel_bytes = c.iterations * 4ull * b.nwords +
+                              (8ull + 4ull * K) * c.total_active +
+                              (4ull + e_bytes + 4ull * K) * c.total_edges +
+                              4ull * K * c.total_updated;
+    st->strategy_hist[KITES_STRATEGY_PLAIN] += c.iterations;
+    st->kernel_launches += launches + 3;
+    if (o.record_iterations) KITES_TRY(record_iterations(g, c, KITES_STRATEGY_PLAIN, st));
+    st->host_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  }
+  if (c.timed_out)
+    return fail(KITES_ERR_TIMEOUT, "no fixed point after %llu iterations",
+                (unsigned long long)c.iterations);
+  return KITES_OK;
+}
+
+template <int OP, typename OffT>
+int dispatch_batch_k(kites_graph *g, const uint32_t *src, uint32_t k, uint32_t *out,
+                     const kites_run_opts &o, kites_run_stats *st) {
+  switch (k) {
+    case 16: return run_batch<OP, OffT, 16>(g, src, out, o, st);
+    case 32: return run_batch<OP, OffT, 32>(g, src, out, o, st);
+    case 64: return run_batch<OP, OffT, 64>(g, src, out, o, st);
+    case 128: return run_batch<OP, OffT, 128>(g, src, out, o, st);
+    case 256: return run_batch<OP, OffT, 256>(g, src, out, o, st);
+    default: return fail(KITES_ERR_INVALID, "batch size %u is not 16, 32, 64, 128 or 256", k);
+  }
+}
+
+template <typename OffT>
+int dispatch_batch(kites_graph *g, int op, const uint32_t *src, uint32_t k, uint32_t *out,
+                   const kites_run_opts &o, kites_run_stats *st) {
+  switch (op) {
+    case OP_SSSP: return dispatch_batch_k<OP_SSSP, OffT>(g, src, k, out, o, st);
+    case OP_SSSP_WRAP: return dispatch_batch_k<OP_SSSP_WRAP, OffT>(g, src, k, out, o, st);
+    case OP_BFS: return dispatch_batch_k<OP_BFS, OffT>(g, src, k, out, o, st);
+    default: return fail(KITES_ERR_INVALID, "batched runs take SSSP, SSSP_WRAP or BFS");
+  }
 }
 
 int check_graph(kites_engine *eng, kites_graph *g) {
@@ -600,6 +1257,15 @@ extern "C" int kites_engine_create(int device, kites_engine **out) {
       st = fail(KITES_ERR_OOM, "pinned scratch allocation failed: %s", cudaGetErrorString(ce));
       break;
     }
+    if ((ce = cudaMalloc((void **)&eng->sel_params, kParams * sizeof(float))) != cudaSuccess) {
+      st = fail(KITES_ERR_OOM, "selector allocation failed: %s", cudaGetErrorString(ce));
+      break;
+    }
+    k_mlp_neutral<<<1, 256, 0, eng->stream>>>(eng->sel_params);
+    if ((ce = cudaStreamSynchronize(eng->stream)) != cudaSuccess) {
+      st = fail(KITES_ERR_CUDA, "selector init failed: %s", cudaGetErrorString(ce));
+      break;
+    }
   } while (0);
   if (st != KITES_OK) {
     kites_engine_destroy(eng);
@@ -616,6 +1282,7 @@ extern "C" int kites_engine_destroy(kites_engine *eng) {
   // Graphs die with their engine; their handles are invalid afterwards.
   while (!eng->graphs.empty()) kites_graph_destroy(eng->graphs.back());
   if (eng->pinned) cudaFreeHost(eng->pinned);
+  if (eng->sel_params) cudaFree(eng->sel_params);
   if (eng->ev0) cudaEventDestroy(eng->ev0);
   if (eng->ev1) cudaEventDestroy(eng->ev1);
   if (eng->kev0) cudaEventDestroy(eng->kev0);
@@ -820,6 +1487,24 @@ extern "C" int kites_process(kites_engine *eng, kites_graph *g, int op,
                   : dispatch_process<uint32_t>(g, op, o, stats);
 }
 
+// Runs `op` with a strategy other than PLAIN from the changed set already in
+// changed[0] (graph values already initialised).
+static int run_strategies(kites_engine *eng, kites_graph *g, int op, const kites_run_opts *opts,
+                          kites_run_stats *stats) {
+  kites_run_opts o = resolve_opts(opts);
+  if (stats) memset(stats, 0, sizeof(*stats));
+  if (g->vsize != 4) return fail(KITES_ERR_UNSUPPORTED, "built-in operators need 4-byte values");
+  if ((op == OP_SSSP || op == OP_SSSP_WRAP) && g->esize != 4)
+    return fail(KITES_ERR_UNSUPPORTED, "SSSP needs 4-byte edge values");
+  if (o.strategy < KITES_STRATEGY_PLAIN || o.strategy >= KITES_STRATEGY_COUNT)
+    return fail(KITES_ERR_INVALID, "unknown strategy %d", o.strategy);
+  if (o.strategy == KITES_STRATEGY_AUTO)
+    return g->off64 ? dispatch_auto<uint64_t>(g, op, o, stats)
+                    : dispatch_auto<uint32_t>(g, op, o, stats);
+  return g->off64 ? dispatch_flex<uint64_t>(g, op, o, stats)
+                  : dispatch_flex<uint32_t>(g, op, o, stats);
+}
+
 extern "C" int kites_sssp(kites_engine *eng, kites_graph *g, int op, uint32_t source,
                           uint32_t *dist_out, const kites_run_opts *opts,
                           kites_run_stats *stats) {
@@ -833,6 +1518,21 @@ extern "C" int kites_sssp(kites_engine *eng, kites_graph *g, int op, uint32_t so
   auto t0 = std::chrono::steady_clock::now();
   k_fill_u32<<<grid_for(g->n), 256, 0, s>>>((uint32_t *)g->V, g->n, kInf);
   KITES_CUDA_TRY(cudaMemsetAsync(g->bitmaps, 0, 4 * g->nwords * 4, s));
+  if (opts && opts->strategy != KITES_STRATEGY_PLAIN) {
+    // Strategy loop: the changed set starts as {source}.
+    k_seed_changed<<<1, 32, 0, s>>>((uint32_t *)g->V, source, g->changed[0]);
+    KITES_CUDA_TRY(cudaGetLastError());
+    int st = run_strategies(eng, g, op, opts, stats);
+    if (st != KITES_OK) return st;
+    if (dist_out) {
+      KITES_CUDA_TRY(cudaMemcpyAsync(dist_out, g->V, g->n_given * 4, cudaMemcpyDefault, s));
+      KITES_CUDA_TRY(cudaStreamSynchronize(s));
+    }
+    if (stats)
+      stats->host_ms = std::chrono::duration<double, std::milli>(
+                           std::chrono::steady_clock::now() - t0).count();
+    return KITES_OK;
+  }
   if (g->off64)
     k_seed_source<uint64_t><<<32, 256, 0, s>>>((uint32_t *)g->V, (const uint64_t *)g->outR,
                                                g->outC, source, g->shift, g->frontier[0]);
@@ -862,9 +1562,14 @@ extern "C" int kites_cc(kites_engine *eng, kites_graph *g, uint32_t *labels_out,
   auto t0 = std::chrono::steady_clock::now();
   k_iota_u32<<<grid_for(g->n), 256, 0, s>>>((uint32_t *)g->V, g->n);
   KITES_CUDA_TRY(cudaMemsetAsync(g->bitmaps, 0, 4 * g->nwords * 4, s));
-  k_all_active<<<grid_for(g->nwords), 256, 0, s>>>(g->frontier[0], g->nbits, g->nwords);
+  const bool strategies = opts && opts->strategy != KITES_STRATEGY_PLAIN;
+  // Every vertex starts active; with a strategy loop every vertex starts
+  // changed (its out-neighbours form the first frontier).
+  k_all_active<<<grid_for(g->nwords), 256, 0, s>>>(strategies ? g->changed[0] : g->frontier[0],
+                                                   strategies ? g->n_given : g->nbits, g->nwords);
   KITES_CUDA_TRY(cudaGetLastError());
-  int st = kites_process(eng, g, OP_CC, opts, stats);
+  int st = strategies ? run_strategies(eng, g, OP_CC, opts, stats)
+                      : kites_process(eng, g, OP_CC, opts, stats);
   if (st != KITES_OK) return st;
   if (labels_out) {
     KITES_CUDA_TRY(cudaMemcpyAsync(labels_out, g->V, g->n_given * 4, cudaMemcpyDefault, s));
@@ -894,7 +1599,135 @@ extern "C" int kites_sssp_batch(kites_engine *eng, kites_graph *g, int op,
                                 const uint32_t *sources, uint32_t k, uint32_t *dist_out,
                                 const kites_run_opts *opts, kites_run_stats *stats) {
   clear_error();
-  (void)eng; (void)g; (void)op; (void)sources; (void)k; (void)dist_out; (void)opts;
-  (void)stats;
-  return fail(KITES_ERR_UNSUPPORTED, "batched SSSP is not built yet");
+  KITES_TRY(check_graph(eng, g));
+  if (!sources) return fail(KITES_ERR_INVALID, "null sources");
+  if (g->esize != 4 && op != OP_BFS) return fail(KITES_ERR_UNSUPPORTED, "SSSP needs 4-byte edge values");
+  if (k != 16 && k != 32 && k != 64 && k != 128 && k != 256)
+    return fail(KITES_ERR_INVALID, "batch size %u is not 16, 32, 64, 128 or 256", k);
+  // Sources are read on the host to reject out-of-range ids before any
+  // kernel indexes with them.
+  uint32_t host_src[256];
+  KITES_CUDA_TRY(cudaMemcpy(host_src, sources, k * 4, cudaMemcpyDefault));
+  for (uint32_t i = 0; i < k; ++i)
+    if (host_src[i] >= g->n_given)
+      return fail(KITES_ERR_INVALID, "source %u (slot %u) out of range", host_src[i], i);
+  kites_run_opts o = resolve_opts(opts);
+  if (stats) memset(stats, 0, sizeof(*stats));
+  return g->off64 ? dispatch_batch<uint64_t>(g, op, host_src, k, dist_out, o, stats)
+                  : dispatch_batch<uint32_t>(g, op, host_src, k, dist_out, o, stats);
+}
+
+// ---- learned selector ------------------------------------------------------------
+
+extern "C" int kites_selector_record(kites_engine *eng, kites_graph *g, int op, uint32_t source,
+                                     float *features, float *times_ms, uint32_t capacity,
+                                     uint32_t *n_records) {
+  clear_error();
+  KITES_TRY(check_graph(eng, g));
+  if (!features || !times_ms || !n_records || capacity == 0)
+    return fail(KITES_ERR_INVALID, "null output or zero capacity");
+  if (op != OP_SSSP && op != OP_BFS && op != OP_CC)
+    return fail(KITES_ERR_INVALID, "recording takes SSSP, BFS or CC");
+  if (op == OP_SSSP && g->esize != 4) return fail(KITES_ERR_UNSUPPORTED, "SSSP needs 4-byte edges");
+  if (op != OP_CC && source >= g->n_given) return fail(KITES_ERR_INVALID, "source out of range");
+  cudaStream_t s = eng->stream;
+  KITES_CUDA_TRY(cudaMemsetAsync(g->bitmaps, 0, 4 * g->nwords * 4, s));
+  if (op == OP_CC) {
+    k_iota_u32<<<grid_for(g->n), 256, 0, s>>>((uint32_t *)g->V, g->n);
+    k_all_active<<<grid_for(g->nwords), 256, 0, s>>>(g->changed[0], g->n_given, g->nwords);
+  } else {
+    k_fill_u32<<<grid_for(g->n), 256, 0, s>>>((uint32_t *)g->V, g->n, kInf);
+    k_seed_changed<<<1, 32, 0, s>>>((uint32_t *)g->V, source, g->changed[0]);
+  }
+  KITES_CUDA_TRY(cudaGetLastError());
+  return g->off64 ? dispatch_record<uint64_t>(g, op, features, times_ms, capacity, n_records)
+                  : dispatch_record<uint32_t>(g, op, features, times_ms, capacity, n_records);
+}
+
+extern "C" int kites_selector_train(kites_engine *eng, const float *features,
+                                    const float *times_ms, uint32_t n, uint32_t epochs,
+                                    float lr, uint64_t seed, float *params_out,
+                                    float *final_loss) {
+  clear_error();
+  if (!eng || !features || !times_ms || n == 0) return fail(KITES_ERR_INVALID, "bad arguments");
+  KITES_TRY(set_device(eng));
+  cudaStream_t s = eng->stream;
+  // Targets: log of each class's time over PLAIN's (host arithmetic).
+  std::vector<float> Y((size_t)n * kClasses);
+  for (uint32_t i = 0; i < n; ++i) {
+    const float t0 = std::max(times_ms[(size_t)i * kClasses], 1e-4f);
+    for (int c = 0; c < kClasses; ++c)
+      Y[(size_t)i * kClasses + c] = logf(std::max(times_ms[(size_t)i * kClasses + c], 1e-4f) / t0);
+  }
+  void *p;
+  const size_t xb = (size_t)n * kFeat * 4, yb = (size_t)n * kClasses * 4;
+  KITES_TRY(dev_alloc(eng, &p, xb + yb + 4 * kParams * 4 + 4));
+  float *dX = (float *)p, *dY = dX + (size_t)n * kFeat, *P = dY + (size_t)n * kClasses;
+  float *G = P + kParams, *M = G + kParams, *Vv = M + kParams, *loss = Vv + kParams;
+  KITES_CUDA_TRY(cudaMemcpyAsync(dX, features, xb, cudaMemcpyDefault, s));
+  KITES_CUDA_TRY(cudaMemcpyAsync(dY, Y.data(), yb, cudaMemcpyHostToDevice, s));
+  KITES_CUDA_TRY(cudaMemsetAsync(G, 0, 3 * kParams * 4 + 4, s));
+  k_mlp_init<<<8, 256, 0, s>>>(P, seed);
+  k_mlp_standardise<<<1, 32, 0, s>>>(dX, n, P);
+  const unsigned blocks = (n + 127) / 128;
+  for (uint32_t e = 1; e <= epochs; ++e) {
+    if (e == epochs) KITES_CUDA_TRY(cudaMemsetAsync(loss, 0, 4, s));
+    k_mlp_grad<<<blocks, 128, 0, s>>>(dX, dY, n, P, G, loss);
+    k_mlp_adam<<<(kParams + 255) / 256, 256, 0, s>>>(P, G, M, Vv, lr, 0.9f, 0.999f, 1e-8f, (int)e);
+  }
+  KITES_CUDA_TRY(cudaGetLastError());
+  KITES_CUDA_TRY(cudaMemcpyAsync(eng->sel_params, P, kParams * 4, cudaMemcpyDeviceToDevice, s));
+  float hloss = 0.f;
+  KITES_CUDA_TRY(cudaMemcpyAsync(&hloss, loss, 4, cudaMemcpyDeviceToHost, s));
+  if (params_out) KITES_CUDA_TRY(cudaMemcpyAsync(params_out, P, kParams * 4, cudaMemcpyDefault, s));
+  KITES_CUDA_TRY(cudaFreeAsync(p, s));
+  KITES_CUDA_TRY(cudaStreamSynchronize(s));
+  if (final_loss) *final_loss = hloss;
+  return KITES_OK;
+}
+
+extern "C" int kites_selector_load(kites_engine *eng, const float *params, uint32_t n_params) {
+  clear_error();
+  if (!eng || !params) return fail(KITES_ERR_INVALID, "null argument");
+  if (n_params != (uint32_t)kParams)
+    return fail(KITES_ERR_INVALID, "selector has %d parameters, got %u", kParams, n_params);
+  KITES_TRY(set_device(eng));
+  KITES_CUDA_TRY(cudaMemcpyAsync(eng->sel_params, params, kParams * 4, cudaMemcpyDefault,
+                                 eng->stream));
+  KITES_CUDA_TRY(cudaStreamSynchronize(eng->stream));
+  return KITES_OK;
+}
+
+extern "C" int kites_selector_save(kites_engine *eng, float *params, uint32_t n_params) {
+  clear_error();
+  if (!eng || !params) return fail(KITES_ERR_INVALID, "null argument");
+  if (n_params != (uint32_t)kParams)
+    return fail(KITES_ERR_INVALID, "selector has %d parameters, got %u", kParams, n_params);
+  KITES_TRY(set_device(eng));
+  KITES_CUDA_TRY(cudaMemcpyAsync(params, eng->sel_params, kParams * 4, cudaMemcpyDefault,
+                                 eng->stream));
+  KITES_CUDA_TRY(cudaStreamSynchronize(eng->stream));
+  return KITES_OK;
+}
+
+extern "C" int kites_graph_set_tpv(kites_graph *g, int strategy) {
+  clear_error();
+  if (!g) return fail(KITES_ERR_INVALID, "null graph");
+  if (strategy != KITES_STRATEGY_TPV1 && strategy != KITES_STRATEGY_TPV4 &&
+      strategy != KITES_STRATEGY_TPV8 && strategy != KITES_STRATEGY_TPV32)
+    return fail(KITES_ERR_INVALID, "not a threads-per-vertex strategy: %d", strategy);
+  if (g->tpv_strategy != strategy) {
+    // Cached AUTO loops captured the old width.
+    for (auto it = g->loops.begin(); it != g->loops.end();) {
+      if (it->first.strategy == 200) {
+        cudaGraphExecDestroy(it->second.second);
+        cudaGraphDestroy(it->second.first);
+        it = g->loops.erase(it);
+      } else {
+        ++it;
+      }
+    }
+    g->tpv_strategy = strategy;
+  }
+  return KITES_OK;
 }

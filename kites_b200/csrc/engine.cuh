@@ -17,6 +17,7 @@ struct kites_engine {
   int sm_count = 0;
   int l2_bytes = 0;
   void *pinned = nullptr;         // small pinned scratch for flag read-backs
+  float *sel_params = nullptr;    // learned selector weights (device), or null
   std::vector<struct kites_graph *> graphs;   // live graphs, destroyed with the engine
 };
 
@@ -74,6 +75,23 @@ struct kites_graph {
   kites_internal::run_counters *ctr = nullptr;
   unsigned long long *rec_active = nullptr;
   unsigned long long *rec_edges = nullptr;
+
+  // Batched multi-source runs (V x K distances), allocated on first use.
+  uint32_t *batchD = nullptr;
+  uint64_t batch_cap = 0;            // elements of batchD
+  uint32_t *bbits = nullptr;         // vertex-level [f0|c0|f1|c1] when vpg > 1
+  uint64_t bnwords = 0;
+  uint32_t batch_chunk_items = 0;    // chunk size of chunk_batch (autotuned)
+  uint32_t *chunk_batch = nullptr;
+  uint64_t nchunks_batch = 0;
+  uint32_t *chunk_out = nullptr;     // vertex-level out-CSR chunks (vpg > 1)
+  uint64_t nchunks_out = 0;
+  uint32_t *d_sources = nullptr;     // 256 source slots
+  uint32_t *queue = nullptr;         // compacted changed queue (PUSH), n slots
+  void *sacc = nullptr;              // selector frontier-count accumulators
+  uint8_t *rec_sel = nullptr;        // selector class per iteration (device)
+  int tpv_strategy = KITES_STRATEGY_TPV8;   // the selector's threads-per-vertex class
+  float auto_margin = -1.f;          // margin the cached AUTO loop was captured with
 
   // PageRank scratch (allocated on first use).
   float *pr_x = nullptr, *pr_y = nullptr, *pr_inv_out = nullptr;

@@ -57,32 +57,119 @@ struct chunk_geom {
 
 // ---- pull -------------------------------------------------------------------
 
+constexpr int kUnroll = 4;  // 32-edge windows in flight per warp
+
+// Per-warp row slice of one chunk: lanes hold (count, first edge) of their
+// row's edges inside the chunk; ex = exclusive prefix of the counts.
+template <typename OffT>
+struct row_slice {
+  uint32_t *ex;
+  OffT *lo;
+};
+
+// Owner lane of virtual edge i (largest j with ex[j] <= i; a lane with no
+// edges shares its ex with the next lane, so the search lands on a lane
+// that owns edges).
+__device__ __forceinline__ uint32_t owner_of(const uint32_t *ex, uint32_t i) {
+  uint32_t j = 0;
+#pragma unroll
+  for (uint32_t step = 16; step; step >>= 1)
+    if (ex[j + step] <= i) j += step;
+  return j;
+}
+
+// Folds p(e) over the slice's `total` virtual edges into acc[owner] with a
+// warp-segmented min.  The policy splits each edge into a streaming load
+// (C, and E when needed) and a dependent value (the V gather), so kUnroll
+// windows of both are in flight before any reduction.
+template <typename OffT, class Policy>
+__device__ __forceinline__ void fold_min(const row_slice<OffT> &rs, uint32_t total,
+                                         uint32_t *acc, const Policy &pol) {
+  const uint32_t lane = lane_id();
+  for (uint32_t base = 0; base < total; base += 32 * kUnroll) {
+    uint32_t own[kUnroll], c[kUnroll], w[kUnroll], p[kUnroll];
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) {
+      const uint32_t i = base + u * 32 + lane;
+      own[u] = 32u;
+      c[u] = 0u;
+      w[u] = 0u;
+      if (i < total) {
+        const uint32_t j = owner_of(rs.ex, i);
+        own[u] = j;
+        pol.load(rs.lo[j] + (OffT)(i - rs.ex[j]), &c[u], &w[u]);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) p[u] = own[u] < 32u ? pol.value(c[u], w[u]) : kInf;
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) {
+      bool head;
+      const uint32_t rm = run_mask(own[u], &head);
+      const uint32_t q = __reduce_min_sync(rm, p[u]);
+      if (head && own[u] < 32u) acc[own[u]] = min(acc[own[u]], q);
+      __syncwarp();
+    }
+  }
+}
+
+// Edge policies.  PullEdges: every in-edge of an active row.
+template <int OP>
+struct pull_edges {
+  const uint32_t *C, *E, *V;
+  __device__ __forceinline__ void load(uint64_t e, uint32_t *c, uint32_t *w) const {
+    *c = __ldcs(C + e);
+    if (op_reads_weights<OP>()) *w = __ldcs(E + e);
+  }
+  __device__ __forceinline__ uint32_t value(uint32_t c, uint32_t w) const {
+    return nbr_comp<OP>(V[c], w);
+  }
+};
+
+// FilteredEdges: only in-edges whose source changed last iteration (bit in U).
+template <int OP>
+struct filtered_edges {
+  const uint32_t *C, *E, *V, *U;
+  __device__ __forceinline__ void load(uint64_t e, uint32_t *c, uint32_t *w) const {
+    const uint32_t src = __ldcs(C + e);
+    const bool on = (U[src >> 5] >> (src & 31u)) & 1u;
+    *c = on ? src : kInf;
+    if (op_reads_weights<OP>() && on) *w = E[e];
+  }
+  __device__ __forceinline__ uint32_t value(uint32_t c, uint32_t w) const {
+    return c == kInf ? kInf : nbr_comp<OP>(V[c], w);
+  }
+};
+
 template <typename OffT>
 struct pull_args {
   chunk_geom<OffT> g;
   const uint32_t *E;
   uint32_t *V;
-  const uint32_t *rd;      // read frontier (bit per vertex or per group)
+  const uint32_t *rd;      // read frontier (bit per vertex or per group); null = all rows
   uint32_t *chg;           // changed rows of the activation adjacency
   uint32_t shift;          // log2(vertex_per_group)
   run_counters *ctr;
+  const uint32_t *U;       // filtered pull: changed set of the previous iteration
 };
 
-template <int OP, typename OffT>
-__global__ void __launch_bounds__(kBlock)
-    k_pull_chunked(pull_args<OffT> a) {
-  if (a.ctr->done) return;
+// The pull iteration over the edge-balanced chunks.  Rows whose frontier
+// bit is set (every row when rd is null) fold their in-edges with the edge
+// policy; a row entirely inside the chunk stores its new value, a row split
+// over chunks merges through atomicMin; updated rows set their bit (vertex
+// or group) in chg.
+template <int OP, typename OffT, bool kFiltered>
+__device__ __forceinline__ void pull_chunks(const pull_args<OffT> &a) {
   __shared__ uint32_t s_ex[kWarpsPerBlock][32];
   __shared__ OffT s_lo[kWarpsPerBlock][32];
   __shared__ uint32_t s_acc[kWarpsPerBlock][32];
   const uint32_t lane = lane_id(), wib = threadIdx.x >> 5;
-  uint32_t *ex = s_ex[wib];
-  OffT *lo_s = s_lo[wib];
+  const row_slice<OffT> rs{s_ex[wib], s_lo[wib]};
   uint32_t *acc_s = s_acc[wib];
-  unsigned long long n_act = 0, n_edges = 0;
+  uint32_t n_act = 0, n_edges = 0;
   const uint64_t stride = (uint64_t)gridDim.x * kWarpsPerBlock;
-  for (uint64_t ch = (uint64_t)blockIdx.x * kWarpsPerBlock + wib;
-       ch < a.g.nchunks; ch += stride) {
+  for (uint64_t ch = (uint64_t)blockIdx.x * kWarpsPerBlock + wib; ch < a.g.nchunks;
+       ch += stride) {
     const int64_t item_lo = (int64_t)(ch * a.g.chunk_items);
     const int64_t item_hi =
         min(item_lo + (int64_t)a.g.chunk_items, (int64_t)a.g.n_items);
@@ -91,10 +178,12 @@ __global__ void __launch_bounds__(kBlock)
     if (v_last >= a.g.n_rows) v_last = a.g.n_rows - 1;
     for (uint64_t vb = v_first & ~31ull; vb <= v_last; vb += 32) {
       const uint64_t v = vb + lane;
-      const uint32_t word = a.rd[(vb >> a.shift) >> 5];
       const bool in_range = v >= v_first && v <= v_last;
-      const bool active =
-          in_range && ((word >> ((v >> a.shift) & 31u)) & 1u);
+      bool active = in_range;
+      if (a.rd) {
+        const uint32_t word = a.rd[(vb >> a.shift) >> 5];
+        active = in_range && ((word >> ((v >> a.shift) & 31u)) & 1u);
+      }
       if (__ballot_sync(kFull, active) == 0) continue;
       uint32_t cnt = 0, old = 0;
       OffT elo = 0;
@@ -107,37 +196,21 @@ __global__ void __launch_bounds__(kBlock)
         elo = (OffT)lo;
         whole = (lo == r0) && (hi == r1);
         const int64_t vpos = (int64_t)v + r0;
-        n_act += (vpos >= item_lo && vpos < item_hi) ? 1 : 0;
+        n_act += (vpos >= item_lo && vpos < item_hi) ? 1u : 0u;
         n_edges += cnt;
         if (cnt) old = a.V[v];
       }
       const uint32_t incl = warp_inclusive_scan(cnt);
       const uint32_t total = __shfl_sync(kFull, incl, 31);
       if (total == 0) continue;
-      ex[lane] = incl - cnt;
-      lo_s[lane] = elo;
+      rs.ex[lane] = incl - cnt;
+      rs.lo[lane] = elo;
       acc_s[lane] = kInf;
       __syncwarp();
-      for (uint32_t base = 0; base < total; base += 32) {
-        const uint32_t i = base + lane;
-        uint32_t owner = 32u, p = kInf;
-        if (i < total) {
-          uint32_t j = 0;
-#pragma unroll
-          for (uint32_t step = 16; step; step >>= 1)
-            if (ex[j + step] <= i) j += step;
-          owner = j;
-          const OffT e = lo_s[j] + (OffT)(i - ex[j]);
-          const uint32_t src = __ldcs(a.g.C + e);
-          const uint32_t w = op_reads_weights<OP>() ? __ldcs(a.E + e) : 0u;
-          p = nbr_comp<OP>(a.V[src], w);
-        }
-        bool head;
-        const uint32_t rm = run_mask(owner, &head);
-        p = __reduce_min_sync(rm, p);
-        if (head && owner < 32u) acc_s[owner] = min(acc_s[owner], p);
-        __syncwarp();
-      }
+      if (kFiltered)
+        fold_min(rs, total, acc_s, filtered_edges<OP>{a.g.C, a.E, a.V, a.U});
+      else
+        fold_min(rs, total, acc_s, pull_edges<OP>{a.g.C, a.E, a.V});
       bool upd = false;
       if (cnt) {
         const uint32_t acc = acc_s[lane];
@@ -159,12 +232,18 @@ __global__ void __launch_bounds__(kBlock)
       }
     }
   }
-  n_act = __reduce_add_sync(kFull, (uint32_t)n_act);
-  n_edges = __reduce_add_sync(kFull, (uint32_t)n_edges);
+  n_act = __reduce_add_sync(kFull, n_act);
+  n_edges = __reduce_add_sync(kFull, n_edges);
   if (lane == 0) {
-    if (n_act) atomicAdd(&a.ctr->active, n_act);
-    if (n_edges) atomicAdd(&a.ctr->edges, n_edges);
+    if (n_act) atomicAdd(&a.ctr->active, (unsigned long long)n_act);
+    if (n_edges) atomicAdd(&a.ctr->edges, (unsigned long long)n_edges);
   }
+}
+
+template <int OP, typename OffT>
+__global__ void __launch_bounds__(kBlock) k_pull_chunked(pull_args<OffT> a) {
+  if (a.ctr->done) return;
+  pull_chunks<OP, OffT, false>(a);
 }
 
 // ---- activation -------------------------------------------------------------
@@ -177,16 +256,17 @@ struct expand_args {
   run_counters *ctr;
 };
 
+// For each changed row, OR the bit of every target into the write frontier;
+// lanes hitting the same target word in a window combine their bits first.
 template <typename OffT>
-__global__ void __launch_bounds__(kBlock)
-    k_expand_chunked(expand_args<OffT> a) {
+__global__ void __launch_bounds__(kBlock) k_expand_chunked(expand_args<OffT> a) {
   if (a.ctr->done) return;
   __shared__ uint32_t s_ex[kWarpsPerBlock][32];
   __shared__ OffT s_lo[kWarpsPerBlock][32];
   const uint32_t lane = lane_id(), wib = threadIdx.x >> 5;
   uint32_t *ex = s_ex[wib];
   OffT *lo_s = s_lo[wib];
-  unsigned long long n_rows = 0, n_edges = 0;
+  uint32_t n_rows = 0, n_edges = 0;
   const uint64_t stride = (uint64_t)gridDim.x * kWarpsPerBlock;
   for (uint64_t ch = (uint64_t)blockIdx.x * kWarpsPerBlock + wib;
        ch < a.g.nchunks; ch += stride) {
@@ -211,7 +291,7 @@ __global__ void __launch_bounds__(kBlock)
         cnt = hi > lo ? (uint32_t)(hi - lo) : 0u;
         elo = (OffT)lo;
         const int64_t rpos = (int64_t)r + r0;
-        n_rows += (rpos >= item_lo && rpos < item_hi) ? 1 : 0;
+        n_rows += (rpos >= item_lo && rpos < item_hi) ? 1u : 0u;
         n_edges += cnt;
       }
       const uint32_t incl = warp_inclusive_scan(cnt);
@@ -220,32 +300,35 @@ __global__ void __launch_bounds__(kBlock)
       ex[lane] = incl - cnt;
       lo_s[lane] = elo;
       __syncwarp();
-      for (uint32_t base = 0; base < total; base += 32) {
-        const uint32_t i = base + lane;
-        uint32_t tword = kFull, tbit = 0;
-        if (i < total) {
-          uint32_t j = 0;
+      for (uint32_t base = 0; base < total; base += 32 * kUnroll) {
+        uint32_t t[kUnroll];
 #pragma unroll
-          for (uint32_t step = 16; step; step >>= 1)
-            if (ex[j + step] <= i) j += step;
-          const OffT e = lo_s[j] + (OffT)(i - ex[j]);
-          const uint32_t t = __ldcs(a.g.C + e);
-          tword = t >> 5;
-          tbit = 1u << (t & 31u);
+        for (int u = 0; u < kUnroll; ++u) {
+          const uint32_t i = base + u * 32 + lane;
+          t[u] = kFull;
+          if (i < total) {
+            const uint32_t j = owner_of(ex, i);
+            t[u] = __ldcs(a.g.C + lo_s[j] + (OffT)(i - ex[j]));
+          }
         }
-        bool head;
-        const uint32_t rm = run_mask(tword, &head);
-        const uint32_t bits = __reduce_or_sync(rm, tbit);
-        if (head && tword != kFull) atomicOr(a.wr + tword, bits);
+#pragma unroll
+        for (int u = 0; u < kUnroll; ++u) {
+          const uint32_t tword = t[u] == kFull ? kFull : (t[u] >> 5);
+          const uint32_t tbit = t[u] == kFull ? 0u : (1u << (t[u] & 31u));
+          bool head;
+          const uint32_t rm = run_mask(tword, &head);
+          const uint32_t bits = __reduce_or_sync(rm, tbit);
+          if (head && tword != kFull) atomicOr(a.wr + tword, bits);
+        }
       }
       __syncwarp();
     }
   }
-  n_rows = __reduce_add_sync(kFull, (uint32_t)n_rows);
-  n_edges = __reduce_add_sync(kFull, (uint32_t)n_edges);
+  n_rows = __reduce_add_sync(kFull, n_rows);
+  n_edges = __reduce_add_sync(kFull, n_edges);
   if (lane == 0) {
-    if (n_rows) atomicAdd(&a.ctr->updated, n_rows);
-    if (n_edges) atomicAdd(&a.ctr->out_edges, n_edges);
+    if (n_rows) atomicAdd(&a.ctr->updated, (unsigned long long)n_rows);
+    if (n_edges) atomicAdd(&a.ctr->out_edges, (unsigned long long)n_edges);
   }
 }
 
@@ -271,6 +354,9 @@ __global__ void k_loop_check(run_counters *c, iter_record rec,
     if (rec.edges) rec.edges[it] = c->edges;
   }
   c->iterations = it + 1;
+  c->last_active = c->active;
+  c->last_edges = c->edges;
+  c->queue_len[0] = 0;
   c->total_active += c->active;
   c->total_edges += c->edges;
   c->total_updated += c->updated;

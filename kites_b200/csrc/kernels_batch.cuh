@@ -1,0 +1,173 @@
+// kernels_batch.cuh -- batched multi-source pull: K sources at once over a
+// V x K vertex-major distance array D (D[v*K + k]).
+//
+// One in-edge read serves all K sources: a warp walks the active vertices
+// of an edge-balanced chunk one at a time; it loads 32 (C, E) pairs with
+// one coalesced load, then for each edge the lanes -- one per source slice
+// -- gather the source vertex's whole K-wide row (64 B .. 1 KB, contiguous)
+// and fold it into their running minima.  K = LPE x VPL with LPE lanes per
+// edge and VPL values per lane (vector loads); for K = 16 two edges are in
+// flight per warp step.  A vertex whose in-edges span several chunks merges
+// its partial rows with atomicMin, like the single-source kernel.
+#pragma once
+#include "kernels.cuh"
+
+namespace kites_internal {
+
+template <int K>
+struct batch_shape {
+  static constexpr int LPE = K >= 32 ? 32 : K;  // lanes per edge
+  static constexpr int VPL = K / LPE;           // values per lane
+  static constexpr int EPW = 32 / LPE;          // edges per warp step
+  static_assert(K == 16 || K == 32 || K == 64 || K == 128 || K == 256, "K");
+};
+
+template <int VPL>
+__device__ __forceinline__ void load_row(const uint32_t *p, uint32_t (&x)[VPL]) {
+  if constexpr (VPL == 1) {
+    x[0] = *p;
+  } else if constexpr (VPL == 2) {
+    const uint2 t = *reinterpret_cast<const uint2 *>(p);
+    x[0] = t.x; x[1] = t.y;
+  } else {
+#pragma unroll
+    for (int q = 0; q < VPL / 4; ++q) {
+      const uint4 t = reinterpret_cast<const uint4 *>(p)[q];
+      x[4 * q] = t.x; x[4 * q + 1] = t.y; x[4 * q + 2] = t.z; x[4 * q + 3] = t.w;
+    }
+  }
+}
+
+template <int VPL>
+__device__ __forceinline__ void store_row(uint32_t *p, const uint32_t (&x)[VPL]) {
+  if constexpr (VPL == 1) {
+    *p = x[0];
+  } else if constexpr (VPL == 2) {
+    *reinterpret_cast<uint2 *>(p) = make_uint2(x[0], x[1]);
+  } else {
+#pragma unroll
+    for (int q = 0; q < VPL / 4; ++q)
+      reinterpret_cast<uint4 *>(p)[q] =
+          make_uint4(x[4 * q], x[4 * q + 1], x[4 * q + 2], x[4 * q + 3]);
+  }
+}
+
+template <typename OffT>
+struct pull_batch_args {
+  chunk_geom<OffT> g;
+  const uint32_t *E;
+  uint32_t *D;            // n x K
+  const uint32_t *rd;     // read frontier (vertex bits)
+  uint32_t *chg;          // changed vertices
+  run_counters *ctr;
+};
+
+template <int OP, typename OffT, int K>
+__global__ void __launch_bounds__(kBlock)
+    k_pull_batch(pull_batch_args<OffT> a) {
+  if (a.ctr->done) return;
+  using S = batch_shape<K>;
+  const uint32_t lane = lane_id(), wib = threadIdx.x >> 5;
+  const uint32_t sub = lane / S::LPE, kl = lane % S::LPE;
+  unsigned long long n_act = 0, n_edges = 0;
+  const uint64_t stride = (uint64_t)gridDim.x * kWarpsPerBlock;
+  for (uint64_t ch = (uint64_t)blockIdx.x * kWarpsPerBlock + wib; ch < a.g.nchunks;
+       ch += stride) {
+    const int64_t item_lo = (int64_t)(ch * a.g.chunk_items);
+    const int64_t item_hi = min(item_lo + (int64_t)a.g.chunk_items, (int64_t)a.g.n_items);
+    const uint64_t v_first = a.g.chunk_v0[ch];
+    uint64_t v_last = a.g.chunk_v0[ch + 1];
+    if (v_last >= a.g.n_rows) v_last = a.g.n_rows - 1;
+    for (uint64_t vb = v_first & ~31ull; vb <= v_last; vb += 32) {
+      uint32_t mask = a.rd[vb >> 5];
+      if (vb < v_first) mask &= kFull << (uint32_t)(v_first - vb);
+      if (v_last - vb < 31) mask &= kFull >> (31u - (uint32_t)(v_last - vb));
+      uint32_t upd_bits = 0;
+      while (mask) {
+        const uint32_t b = __ffs(mask) - 1;
+        mask &= mask - 1;
+        const uint64_t v = vb + b;
+        const int64_t r0 = (int64_t)a.g.R[v], r1 = (int64_t)a.g.R[v + 1];
+        const int64_t lo = max(r0, item_lo - (int64_t)v - 1);
+        const int64_t hi = min(r1, item_hi - (int64_t)v - 1);
+        const int64_t vpos = (int64_t)v + r0;
+        if (lane == 0) n_act += (vpos >= item_lo && vpos < item_hi) ? 1 : 0;
+        if (hi <= lo) continue;
+        if (lane == 0) n_edges += (uint64_t)(hi - lo);
+        const bool whole = lo == r0 && hi == r1;
+        uint32_t acc[S::VPL];
+#pragma unroll
+        for (int q = 0; q < S::VPL; ++q) acc[q] = kInf;
+        for (int64_t tile = lo; tile < hi; tile += 32) {
+          const int64_t t = tile + lane;
+          const uint32_t ntile = (uint32_t)min((int64_t)32, hi - tile);
+          uint32_t cC = 0, cE = 0;
+          if (t < hi) {
+            cC = __ldcs(a.g.C + t);
+            if (op_reads_weights<OP>()) cE = __ldcs(a.E + t);
+          }
+#pragma unroll 4
+          for (uint32_t jj = 0; jj < ntile; jj += S::EPW) {
+            const uint32_t j = jj + sub;
+            const uint32_t u = __shfl_sync(kFull, cC, j & 31u);
+            const uint32_t w = __shfl_sync(kFull, cE, j & 31u);
+            if (j < ntile) {
+              uint32_t row[S::VPL];
+              load_row<S::VPL>(a.D + (uint64_t)u * K + kl * S::VPL, row);
+#pragma unroll
+              for (int q = 0; q < S::VPL; ++q) acc[q] = min(acc[q], nbr_comp<OP>(row[q], w));
+            }
+          }
+        }
+        if (S::EPW == 2) {
+#pragma unroll
+          for (int q = 0; q < S::VPL; ++q) acc[q] = min(acc[q], __shfl_xor_sync(kFull, acc[q], 16));
+        }
+        bool lane_upd = false;
+        if (sub == 0) {
+          uint32_t *dv = a.D + v * K + kl * S::VPL;
+          uint32_t cur[S::VPL];
+          load_row<S::VPL>(dv, cur);
+          if (whole) {
+            bool any = false;
+#pragma unroll
+            for (int q = 0; q < S::VPL; ++q) {
+              if (acc[q] < cur[q]) { cur[q] = acc[q]; any = true; }
+            }
+            if (any) { store_row<S::VPL>(dv, cur); lane_upd = true; }
+          } else {
+#pragma unroll
+            for (int q = 0; q < S::VPL; ++q)
+              if (acc[q] < cur[q] && acc[q] < atomicMin(dv + q, acc[q])) lane_upd = true;
+          }
+        }
+        if (__any_sync(kFull, lane_upd)) upd_bits |= 1u << b;
+      }
+      if (upd_bits && lane == 0) {
+        atomicOr(a.chg + (vb >> 5), upd_bits);
+        a.ctr->update_flag = 1u;
+      }
+    }
+  }
+  if (lane == 0) {
+    if (n_act) atomicAdd(&a.ctr->active, n_act);
+    if (n_edges) atomicAdd(&a.ctr->edges, n_edges);
+  }
+}
+
+// D = INF everywhere, D[s_k * K + k] = 0, frontier bits for every
+// out-neighbour of every source.
+template <typename OffT>
+__global__ void k_seed_batch(uint32_t *D, uint32_t K, const uint32_t *__restrict__ sources,
+                             const OffT *__restrict__ outR, const uint32_t *__restrict__ outC,
+                             uint32_t *frontier) {
+  const uint32_t k = blockIdx.x;
+  const uint32_t s = sources[k];
+  if (threadIdx.x == 0) D[(uint64_t)s * K + k] = 0u;
+  for (OffT i = outR[s] + threadIdx.x; i < outR[s + 1]; i += blockDim.x) {
+    const uint32_t t = outC[i];
+    atomicOr(frontier + (t >> 5), 1u << (t & 31u));
+  }
+}
+
+}  // namespace kites_internal

@@ -238,3 +238,55 @@ def test_repeated_runs_and_pool_reuse(engine, cfg1_edges):
         g.close()
     _, _, pool = engine.mem_usage()
     assert pool > 0
+
+
+@pytest.mark.parametrize("k", [16, 32, 64, 128, 256])
+@pytest.mark.parametrize("op", [capi.OP_SSSP, capi.OP_BFS])
+def test_batched_sources_match_single_source(engine, k, op):
+    n = 1 << 13
+    s, d, w = capi.gen_rmat(13, 16 << 13, seed=21)
+    R, C, E = capi.csc_from_edges(n, s, d, w)
+    g = capi.Graph(engine, R, C, E)
+    rng = np.random.default_rng(k)
+    srcs = rng.choice(n, size=k, replace=False).astype(np.uint32)
+    dist, st = g.sssp_batch(srcs, op=op)
+    assert dist.shape == (n, k)
+    oop = O.OP_SSSP_SAT if op == capi.OP_SSSP else O.OP_BFS_SAT
+    for j in range(0, k, max(1, k // 16)):
+        V0 = np.full(n, INF, np.uint32)
+        V0[srcs[j]] = 0
+        want, _ = O.sanity_check(R, C, E, V0, op=oop)
+        np.testing.assert_array_equal(dist[:, j], want, err_msg=f"source slot {j}")
+    assert st.iterations > 1
+
+
+@pytest.mark.parametrize("device_loop", [0, 1])
+def test_batched_cfg1_golden_and_vpg_graph(engine, golden, cfg1_edges, device_loop):
+    s, d, w = cfg1_edges
+    R, C, E = capi.csc_from_edges(7115, s, d, w)
+    g = capi.Graph(engine, R, C, E)
+    srcs = np.array([0, 4321] + list(range(100, 114)), np.uint32)
+    dist, _ = g.sssp_batch(srcs, opts=capi.default_opts(device_loop=device_loop))
+    np.testing.assert_array_equal(dist[:, 0], golden["cfg1_sssp"][:7115])
+    np.testing.assert_array_equal(dist[:, 1], golden["cfg1_sssp_src4321"][:7115])
+    # The same through a vpg = 4 upload (vertex-level activation in batches).
+    hg = O.build_host_graph(s, d, w, vpg=4, init="source", source=0, inf=INF)
+    g4 = upload_host_graph(engine, hg)
+    dist4, _ = g4.sssp_batch(srcs)
+    np.testing.assert_array_equal(dist4[:, :], dist)
+
+
+def test_batch_rejects_bad_input(engine, cfg1_edges):
+    s, d, w = cfg1_edges
+    R, C, E = capi.csc_from_edges(7115, s, d, w)
+    g = capi.Graph(engine, R, C, E)
+    with pytest.raises(capi.KitesError) as ei:
+        g.sssp_batch(np.arange(20, dtype=np.uint32))
+    assert ei.value.status == capi.ERR_INVALID
+    bad = np.arange(16, dtype=np.uint32)
+    bad[3] = 7115
+    with pytest.raises(capi.KitesError) as ei:
+        g.sssp_batch(bad)
+    assert ei.value.status == capi.ERR_INVALID
+    dist, _ = g.sssp_batch(np.arange(16, dtype=np.uint32))  # still usable
+    assert dist[0, 0] == 0

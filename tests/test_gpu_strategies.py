@@ -1,0 +1,124 @@
+"""Per-iteration strategies and the learned selector: every strategy, and
+every mix of strategies the selector picks, reaches the oracle's fixed
+point bit for bit."""
+import numpy as np
+import pytest
+
+from kites_b200 import capi
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+INF = O.INF32
+STRATEGIES = [capi.STRATEGY_PLAIN, capi.STRATEGY_PUSH, capi.STRATEGY_PULL_ALL,
+              capi.STRATEGY_TPV1, capi.STRATEGY_TPV4, capi.STRATEGY_TPV8,
+              capi.STRATEGY_TPV32, capi.STRATEGY_AUTO]
+
+
+def graphs():
+    s, d, w = capi.gen_rmat(14, 16 << 14, seed=31)
+    yield "rmat14", 1 << 14, s, d, w
+    s, d, w = capi.gen_grid(48, seed=3)
+    yield "grid48", 48 * 48, s, d, w
+    s, d, w = capi.gen_er(5000, 30000, seed=4)
+    yield "er5k", 5000, s, d, w
+
+
+GRAPHS = list(graphs())
+
+
+@pytest.fixture(scope="module")
+def uploaded(engine):
+    out = {}
+    for name, n, s, d, w in GRAPHS:
+        R, C, E = capi.csc_from_edges(n, s, d, w)
+        out[name] = (capi.Graph(engine, R, C, E), R, C, E, n)
+    yield out
+    for g, *_ in out.values():
+        g.close()
+
+
+@pytest.mark.parametrize("strategy", STRATEGIES)
+@pytest.mark.parametrize("device_loop", [0, 1])
+@pytest.mark.parametrize("name", [g[0] for g in GRAPHS])
+def test_strategy_sssp_bfs(uploaded, strategy, device_loop, name):
+    g, R, C, E, n = uploaded[name]
+    o = capi.default_opts(strategy=strategy, device_loop=device_loop)
+    for op, oop in [(capi.OP_SSSP, O.OP_SSSP_SAT), (capi.OP_BFS, O.OP_BFS_SAT)]:
+        src = 7
+        dist, st = g.sssp(src, op=op, opts=o)
+        V0 = np.full(n, INF, np.uint32)
+        V0[src] = 0
+        want, _ = O.sanity_check(R, C, E, V0, op=oop)
+        np.testing.assert_array_equal(dist, want)
+        assert sum(st.strategy_hist) == st.iterations
+
+
+@pytest.mark.parametrize("strategy", [capi.STRATEGY_PUSH, capi.STRATEGY_PULL_ALL,
+                                      capi.STRATEGY_TPV8, capi.STRATEGY_AUTO])
+def test_strategy_cc(engine, cfg1_edges, golden, strategy):
+    s, d, _ = cfg1_edges
+    ss, tt = np.concatenate([s, d]), np.concatenate([d, s])
+    k = np.unique(ss.astype(np.uint64) << np.uint64(32) | tt)
+    ss = (k >> np.uint64(32)).astype(np.uint32)
+    tt = (k & np.uint64(0xFFFFFFFF)).astype(np.uint32)
+    R, C, _ = capi.csc_from_edges(7115, ss, tt)
+    g = capi.Graph(engine, R, C, None)
+    labels, _ = g.cc(opts=capi.default_opts(strategy=strategy))
+    np.testing.assert_array_equal(labels, golden["cfg1_cc"][:7115])
+
+
+def forced_selector(cls):
+    """Selector weights that always predict class `cls` far below PLAIN."""
+    P = np.zeros(capi.SELECTOR_PARAMS, np.float32)
+    P[capi.SEL_OFF["std"]:capi.SEL_OFF["std"] + 12] = 1.0
+    b3 = capi.SEL_OFF["b3"]
+    P[b3:b3 + 4] = 0.0
+    if cls:
+        P[b3 + cls] = -5.0
+    return P
+
+
+@pytest.mark.parametrize("cls", [0, 1, 2, 3])
+@pytest.mark.parametrize("device_loop", [0, 1])
+def test_selector_switch_takes_each_class(engine, uploaded, cls, device_loop):
+    g, R, C, E, n = uploaded["rmat14"]
+    engine.selector_load(forced_selector(cls))
+    try:
+        o = capi.default_opts(strategy=capi.STRATEGY_AUTO, device_loop=device_loop)
+        dist, st = g.sssp(3, opts=o)
+        V0 = np.full(n, INF, np.uint32)
+        V0[3] = 0
+        want, _ = O.sanity_check(R, C, E, V0, op=O.OP_SSSP_SAT)
+        np.testing.assert_array_equal(dist, want)
+        strat = capi.CLASS_STRATEGY[cls] if cls != 3 else capi.STRATEGY_TPV8
+        assert st.strategy_hist[strat] == st.iterations, list(st.strategy_hist)
+    finally:
+        engine.selector_load(forced_selector(0))
+
+
+def test_selector_record_train_and_run(engine, uploaded):
+    g, R, C, E, n = uploaded["rmat14"]
+    X, T = [], []
+    for src in (1, 2, 5, 9):
+        x, t = g.selector_record(capi.OP_SSSP, src, capacity=256)
+        assert x.shape[0] >= 3 and np.all(t > 0)
+        X.append(x)
+        T.append(t)
+    X, T = np.concatenate(X), np.concatenate(T)
+    params, loss = engine.selector_train(X, T, epochs=400, lr=3e-3, seed=2)
+    assert np.isfinite(loss) and params.shape == (capi.SELECTOR_PARAMS,)
+    np.testing.assert_array_equal(engine.selector_save(), params)
+    # Whatever it picks, the result is the fixed point.
+    o = capi.default_opts(strategy=capi.STRATEGY_AUTO, selector_margin=0.0)
+    dist, st = g.sssp(11, opts=o)
+    V0 = np.full(n, INF, np.uint32)
+    V0[11] = 0
+    want, _ = O.sanity_check(R, C, E, V0, op=O.OP_SSSP_SAT)
+    np.testing.assert_array_equal(dist, want)
+    engine.selector_load(forced_selector(0))
+
+
+def test_selector_rejects_bad_sizes(engine):
+    with pytest.raises(capi.KitesError):
+        engine.selector_load(np.zeros(10, np.float32))
