@@ -5,18 +5,22 @@
 Workload (default): directed R-MAT scale 24 -- 16,777,216 vertices,
 268,435,456 edges after removing self-loops and duplicate pairs
 (a,b,c,d = 0.57,0.19,0.19,0.05, seed 1), uint32 weights uniform in [1,255].
-One step = single-source SSSP from each of 16 seeded sources.  The metric is
-Graph500-style GTEPS: the sum over sources of edges whose source endpoint is
-reached, divided by the time.  The CSC (2.2 GB) is larger than L2, so every
-step streams it from HBM.
+One step = SSSP from 64 seeded sources.  The metric is Graph500-style
+GTEPS: the sum over sources of edges whose source endpoint is reached,
+divided by the time.  The CSC (2.2 GB) and the 64-wide distance array
+(4.3 GB) are larger than L2, so every step streams them from HBM.
 
-Multi-GPU: replicas only -- each rank runs its own 16 sources on its own
-copy of the graph (weak scaling); torch.distributed carries only the
-barrier and the max-over-ranks of the timings.
+The headline value runs the 64 sources as batches (V x K vertex-major
+distances, one pass per in-edge for all K sources); the same sources run
+one at a time through the plain kernel are timed alongside ("plain").
+
+Multi-GPU: replicas only -- each rank runs its own sources on its own copy
+of the graph (weak scaling); torch.distributed carries only the barrier and
+the max-over-ranks of the timings.
 
 --impl reference times farkhor/KiTES's own CPU vertex-centric loop
 (kites::sanity_check, compiled from the reference headers into
-oracle/_ref/libref_harness.so) on a bounded sample of the same workload.
+oracle/_ref/libref_harness.so) on a bounded sample of the workload.
 """
 from __future__ import annotations
 
@@ -47,10 +51,13 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--scale", type=int, default=24)
     ap.add_argument("--edge-factor", type=int, default=16)
-    ap.add_argument("--sources", type=int, default=16)
+    ap.add_argument("--sources", type=int, default=64)
+    ap.add_argument("--batch", type=int, default=64, choices=[16, 32, 64, 128, 256])
+    ap.add_argument("--strategy", default="plain", choices=["plain", "auto"])
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--ref-sample-scale", type=int, default=20)
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
@@ -74,7 +81,7 @@ def pick_sources(outdeg, count, seed, offset=0):
     """Seeded sources among vertices with out-edges (SplitMix64 draws)."""
     cand = np.flatnonzero(outdeg > 0)
     out = []
-    k = offset * 1000
+    k = offset * 100000
     mask = (1 << 64) - 1
     while len(out) < count:
         z = (seed * 0x9E3779B97F4A7C15 + (k + 1) * 0xBF58476D1CE4E5B9) & mask
@@ -102,6 +109,7 @@ class ClockSampler:
     def __init__(self, device):
         self.device = device
         self.proc = None
+        self.lines = []
 
     def __enter__(self):
         try:
@@ -115,7 +123,6 @@ class ClockSampler:
         return self
 
     def __exit__(self, *exc):
-        self.lines = []
         if self.proc is not None:
             time.sleep(0.25)
             self.proc.terminate()
@@ -129,7 +136,7 @@ class ClockSampler:
     def summary(self):
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in getattr(self, "lines", []):
+        for ln in self.lines:
             f = [x.strip() for x in ln.split(",")]
             if len(f) < 9:
                 continue
@@ -157,23 +164,13 @@ def dist_setup(backend):
     return world, rank, local
 
 
-def max_over_ranks(x, world, device):
+def reduce_over_ranks(x, world, device, op):
     if world == 1:
         return x
     import torch
     import torch.distributed as tdist
     t = torch.tensor([x], dtype=torch.float64, device=device)
-    tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
-    return float(t.item())
-
-
-def sum_over_ranks(x, world, device):
-    if world == 1:
-        return x
-    import torch
-    import torch.distributed as tdist
-    t = torch.tensor([x], dtype=torch.float64, device=device)
-    tdist.all_reduce(t, op=tdist.ReduceOp.SUM)
+    tdist.all_reduce(t, op=getattr(tdist.ReduceOp, op))
     return float(t.item())
 
 
@@ -188,8 +185,8 @@ def barrier(world):
 # ---------------------------------------------------------------------------
 
 def ref_sample(scale, seed, sources=1):
-    """Bounded sample for the reference's single-thread loop: SSSP from one
-    seeded source on an R-MAT of `scale` with the same generator and
+    """Bounded sample for the reference's single-thread loop: SSSP from
+    seeded sources on an R-MAT of `scale` with the same generator and
     parameters as the benchmark graph."""
     n, m, R, C, E, outdeg = make_graph(scale, 16, seed)
     if R[-1] > 0xFFFFFFFF:
@@ -201,7 +198,7 @@ def ref_sample(scale, seed, sources=1):
 def time_reference(lib, n, m, R32, C, E, outdeg, src):
     V = np.full(n, 0xFFFFFFFF, np.uint32)
     V[src] = 0
-    p = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+    p = lambda a: a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
     secs = lib.ref_sanity_check_csc(0, n, m, p(V), p(R32), p(C), p(E))
     if secs < 0:
         raise RuntimeError("reference loop failed")
@@ -216,6 +213,12 @@ def load_ref_lib():
     lib.ref_sanity_check_csc.argtypes = [ctypes.c_int, ctypes.c_uint64, ctypes.c_uint64] + \
         [ctypes.c_void_p] * 4
     return lib
+
+
+def ref_sample_text(scale, n, m):
+    return (f"single-source SSSP on R-MAT scale {scale} ({n} vertices, {m} edges, same "
+            f"generator and parameters as the benchmark graph), one seeded source per "
+            f"step, farkhor/KiTES kites::sanity_check loop, 1 thread")
 
 
 def run_reference(args):
@@ -239,9 +242,6 @@ def run_reference(args):
             edges.append(me)
     total_t = sum(times)
     value = sum(edges) / total_t / 1e9
-    sample = (f"single-source SSSP per step on R-MAT scale {args.ref_sample_scale} "
-              f"({n} vertices, {m} edges, same generator/parameters), one seeded "
-              f"source per step, reference kites::sanity_check loop, 1 thread")
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
@@ -249,7 +249,7 @@ def run_reference(args):
         "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
         "config": config,
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
-                         "sample": sample},
+                         "sample": ref_sample_text(args.ref_sample_scale, n, m)},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }))
@@ -262,8 +262,9 @@ def workload_config(args):
             "graph": f"directed R-MAT scale {args.scale}: {n} vertices, "
                      f"{args.edge_factor * n} edges, a,b,c=0.57,0.19,0.19, seed {args.seed}, "
                      f"uint32 weights U[1,255], no self-loops/duplicates",
-            "sources_per_step": args.sources, "strategy": "plain",
-            "l2": "inputs larger than L2 (CSC 2.2 GB vs 126 MB L2)",
+            "sources_per_step": args.sources, "batch": args.batch,
+            "strategy": args.strategy,
+            "l2": "inputs larger than L2 (CSC 2.2 GB, distances 4.3 GB vs 126 MB L2)",
             "parallelism": f"replicas{args.gpus}"}
 
 
@@ -285,93 +286,122 @@ def run_ours(args):
     del C, E
     stream = torch.cuda.ExternalStream(g.device_view().stream, device=device)
     srcs = pick_sources(outdeg, args.sources, args.seed, offset=rank)
-    opts = capi.default_opts(device_loop=1)
+    K = args.batch
+    if args.sources % K:
+        raise SystemExit("--sources must be a multiple of --batch")
+    groups = [srcs[i:i + K] for i in range(0, len(srcs), K)]
+    strat = capi.STRATEGY_PLAIN if args.strategy == "plain" else capi.STRATEGY_AUTO
+    bopts = capi.default_opts(device_loop=1, strategy=strat)
+    lib = capi.load()
 
-    # Warm-up (also fixes the reached-edge count per source).
-    reached = np.zeros(len(srcs), np.int64)
-    host_dist = np.empty(n, np.uint32)
-    for w in range(args.warmup):
-        for i, s in enumerate(srcs):
-            dist, st = g.sssp(int(s), out=host_dist if w == 0 else False, opts=opts)
-            if w == 0:
-                reached[i] = reached_edges(dist, outdeg)
+    def batched_step():
+        launches = 0
+        for grp in groups:
+            st = capi.RunStats()
+            capi._check(lib.kites_sssp_batch(eng._h, g._h, capi.OP_SSSP, capi._p(grp), K, None,
+                                             ctypes.byref(bopts), ctypes.byref(st)))
+            launches += st.kernel_launches
+        return launches
+
+    # Reached edges per source (fixes the units of a step), from single runs.
+    host = np.empty(n, np.uint32)
+    reached = np.array([reached_edges(g.sssp(int(s), out=host)[0], outdeg) for s in srcs])
     units_per_step = int(reached.sum())
+    for _ in range(args.warmup):
+        batched_step()
 
     # Timed region: K steps, inputs resident, events on the engine stream.
-    launches = 0
     barrier(world)
     torch.cuda.synchronize()
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
+    launches = 0
     with ClockSampler(local) as clk:
         ev0.record(stream)
-        iters = 0
         for _ in range(args.steps):
-            for s in srcs:
-                _, st = g.sssp(int(s), out=False, opts=opts)
-                launches += st.kernel_launches
-                iters += st.iterations
+            launches += batched_step()
         ev1.record(stream)
         torch.cuda.synchronize()
     barrier(world)
     ms = ev0.elapsed_time(ev1)
-    ms_max = max_over_ranks(ms, world, device)
-    total_units = sum_over_ranks(units_per_step * args.steps, world, device)
+    ms_max = reduce_over_ranks(ms, world, device, "MAX")
+    total_units = reduce_over_ranks(units_per_step * args.steps, world, device, "SUM")
     value = total_units / (ms_max * 1e-3) / 1e9
 
-    # Roofline of the dominant kernel (k_pull_chunked): host loop with CUDA
-    # events around every pull launch, one pass over the step's sources.
-    kopts = capi.default_opts(device_loop=0, time_kernels=1)
-    k_ms, k_bytes, k_launch, all_bytes, dev_ms = 0.0, 0, 0, 0, 0.0
-    for s in srcs:
-        _, st = g.sssp(int(s), out=False, opts=kopts)
-        k_ms += st.pull_kernel_ms
-        k_bytes += st.pull_kernel_bytes
-        k_launch += st.pull_kernel_launches
-    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) \
-        if os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
-    peak = peaks.get("hbm_gbs", 6650.0)
-    achieved = k_bytes / (k_ms * 1e-3) / 1e9 if k_ms > 0 else None
-    traffic = None
-    prof = os.path.join(ROOT, "profiles", "pull_traffic.json")
-    if os.path.exists(prof):
-        try:
-            t = json.load(open(prof))
-            if t.get("workload") == f"rmat{args.scale}":
-                traffic = t.get("bytes_per_launch")
-        except (OSError, ValueError):
-            traffic = None
+    # Plain kernel, the same sources one at a time.
+    plain = None
+    popts = capi.default_opts(device_loop=1)
+    if not args.no_plain:
+        for s in srcs[:4]:
+            g.sssp(int(s), out=False, opts=popts)
+        barrier(world)
+        torch.cuda.synchronize()
+        p0 = torch.cuda.Event(enable_timing=True)
+        p1 = torch.cuda.Event(enable_timing=True)
+        p0.record(stream)
+        for s in srcs:
+            g.sssp(int(s), out=False, opts=popts)
+        p1.record(stream)
+        torch.cuda.synchronize()
+        pms = reduce_over_ranks(p0.elapsed_time(p1), world, device, "MAX")
+        plain = {"value": reduce_over_ranks(units_per_step, world, device, "SUM") /
+                 (pms * 1e-3) / 1e9, "unit": UNIT, "ms_per_step": pms}
 
-    # End-to-end through the C ABI: results copied to pinned host memory
-    # every run (the step's inputs are the 16 source ids).
+    # Rooflines of the dominant kernels, timed live with CUDA events around
+    # every launch (host loop): k_pull_batch for the headline, k_pull_chunked
+    # for the plain kernel's traversal phase.
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    peaks = json.load(open(peaks_path)) if os.path.exists(peaks_path) else {}
+    peak = peaks.get("hbm_gbs", 6650.0)
+    kopts = capi.default_opts(device_loop=0, time_kernels=1)
+    st = capi.RunStats()
+    capi._check(lib.kites_sssp_batch(eng._h, g._h, capi.OP_SSSP, capi._p(groups[0]), K, None,
+                                     ctypes.byref(kopts), ctypes.byref(st)))
+    b_ach = st.pull_kernel_bytes / (st.pull_kernel_ms * 1e-3) / 1e9
+    k_ms, k_bytes, k_launch = 0.0, 0, 0
+    for s in srcs[:8]:
+        _, pst = g.sssp(int(s), out=False, opts=kopts)
+        k_ms += pst.pull_kernel_ms
+        k_bytes += pst.pull_kernel_bytes
+        k_launch += pst.pull_kernel_launches
+    p_ach = k_bytes / (k_ms * 1e-3) / 1e9
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(prof):
+        t = json.load(open(prof))
+        traffic = t.get(f"k_pull_batch_K{K}_rmat{args.scale}")
+    src_note = "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback 6.65 TB/s"
+
+    # End to end through the C ABI: every batch's V x K distances copied to
+    # pinned host memory (the step's inputs are its source ids).
     e2e = None
     if not args.no_e2e:
-        pinned = torch.empty(n, dtype=torch.int32, pin_memory=True)
+        pinned = torch.empty((n, K), dtype=torch.int32, pin_memory=True)
         barrier(world)
         torch.cuda.synchronize()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         for _ in range(args.steps):
-            for s in srcs:
-                g.sssp(int(s), out=pinned, opts=opts)
+            for grp in groups:
+                capi._check(lib.kites_sssp_batch(eng._h, g._h, capi.OP_SSSP, capi._p(grp), K,
+                                                 capi._p(pinned), ctypes.byref(bopts), None))
         e1.record(stream)
         torch.cuda.synchronize()
-        e_ms = max_over_ranks(e0.elapsed_time(e1), world, device)
+        e_ms = reduce_over_ranks(e0.elapsed_time(e1), world, device, "MAX")
         e2e = {"value": total_units / (e_ms * 1e-3) / 1e9, "unit": UNIT,
                "h2d_bytes_per_step": 4 * len(srcs),
                "d2h_bytes_per_step": 4 * n * len(srcs)}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        lib = load_ref_lib()
-        if lib is not None:
+        rlib = load_ref_lib()
+        if rlib is not None:
             n2, m2, R32, C2, E2, od2, s2 = ref_sample(args.ref_sample_scale, args.seed, 1)
-            secs, me = time_reference(lib, n2, m2, R32, C2, E2, od2, int(s2[0]))
+            secs, me = time_reference(rlib, n2, m2, R32, C2, E2, od2, int(s2[0]))
             cpu = {"value": me / secs / 1e9, "unit": UNIT, "cores": 1, "kind": "reference",
-                   "sample": f"single-source SSSP on R-MAT scale {args.ref_sample_scale} "
-                             f"({n2} vertices, {m2} edges, same generator/parameters), "
-                             f"reference kites::sanity_check loop, 1 thread, {secs:.2f} s"}
+                   "sample": ref_sample_text(args.ref_sample_scale, n2, m2) +
+                   f" ({secs:.2f} s)"}
 
     if rank == 0:
         line = {
@@ -380,15 +410,19 @@ def run_ours(args):
             "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
             "config": workload_config(args),
-            "clocks": {k: v for k, v in clk.summary().items()},
+            "clocks": clk.summary(),
             "e2e": e2e,
             "gpu_launches": int(launches),
-            "iterations_per_source": iters / (args.steps * len(srcs)),
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak,
-                         "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
-                         "traffic": traffic, "kernel": "k_pull_chunked",
-                         "launches": k_launch, "peak_source": "MEASURED_PEAKS.json hbm_gbs"
-                         if peaks else "fallback 6.65 TB/s"},
+            "plain": plain,
+            "speedup_vs_plain": (value / plain["value"]) if plain else None,
+            "roofline": {"bound": "hbm", "achieved": b_ach, "peak": peak, "unit": "GB/s",
+                         "frac": b_ach / peak, "traffic": traffic,
+                         "kernel": f"k_pull_batch<SSSP,K={K}>",
+                         "launches": int(st.pull_kernel_launches), "peak_source": src_note},
+            "roofline_plain": {"bound": "hbm", "achieved": p_ach, "peak": peak,
+                               "unit": "GB/s", "frac": p_ach / peak,
+                               "kernel": "k_pull_chunked<SSSP>", "launches": k_launch,
+                               "peak_source": src_note},
             "cpu_baseline": cpu,
         }
         print(json.dumps(line))

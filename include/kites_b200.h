@@ -209,6 +209,15 @@ int kites_sssp_batch(kites_engine *eng, kites_graph *g, int op,
                      const uint32_t *sources, uint32_t k, uint32_t *dist_out,
                      const kites_run_opts *opts, kites_run_stats *stats);
 
+/* Multi-seed SSSP/BFS: every seed starts at 0 (one super-source).  On a
+ * disjoint union of graphs with one seed per member this runs a whole batch
+ * of independent graphs in one device loop (multi-graph batching); each
+ * member's distances equal its own single-source result.  No reference
+ * counterpart beyond process() itself. */
+int kites_sssp_multi_seed(kites_engine *eng, kites_graph *g, int op, const uint32_t *seeds,
+                          uint64_t n_seeds, uint32_t *dist_out, const kites_run_opts *opts,
+                          kites_run_stats *stats);
+
 /* Min-label connected components: V[v] = v, every vertex active. */
 int kites_cc(kites_engine *eng, kites_graph *g, uint32_t *labels_out,
              const kites_run_opts *opts, kites_run_stats *stats);
@@ -263,6 +272,14 @@ int kites_gen_er(uint64_t n_vertices, uint64_t n_edges, uint64_t seed,
 /* side x side 4-neighbour grid, both directions, 2*2*side*(side-1) edges. */
 int kites_gen_grid(uint32_t side, uint64_t seed, uint32_t w_lo, uint32_t w_hi,
                    uint32_t *src, uint32_t *dst, uint32_t *w);
+/* Disjoint union of n_graphs R-MAT graphs for multi-graph batches: graph i
+ * has V_i log-uniform in [v_min, v_max], edge factor uniform in
+ * [ef_min, ef_max]; its vertex ids start at vertex_offsets[i] and its edges
+ * at edge_offsets[i] (both n_graphs + 1 entries).  src == NULL: sizes only. */
+int kites_gen_rmat_union(uint32_t n_graphs, uint64_t seed, uint32_t v_min, uint32_t v_max,
+                         uint32_t ef_min, uint32_t ef_max, uint32_t w_lo, uint32_t w_hi,
+                         uint64_t *vertex_offsets, uint64_t *edge_offsets, uint32_t *src,
+                         uint32_t *dst, uint32_t *w);
 /* Edge list -> CSC keyed by destination, rows sorted by source (ties in
  * input order), graph_raw.h:102,131 semantics; R has n_vertices+1 entries. */
 int kites_csc_from_edges(uint64_t n_vertices, uint64_t n_edges,

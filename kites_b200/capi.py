@@ -36,6 +36,7 @@ EXPORTED = [
     "kites_cc", "kites_pagerank", "kites_gen_rmat", "kites_gen_er", "kites_gen_grid",
     "kites_csc_from_edges", "kites_selector_record", "kites_selector_train",
     "kites_selector_load", "kites_selector_save", "kites_graph_set_tpv",
+    "kites_sssp_multi_seed", "kites_gen_rmat_union",
 ]
 SELECTOR_FEATURES, SELECTOR_CLASSES, SELECTOR_PARAMS = 12, 4, 1628
 # Parameter layout of the selector MLP (offsets into the 1628 floats).
@@ -145,6 +146,10 @@ def load(path: str = LIB_PATH):
         "kites_selector_load": (c_int, [vp, vp, u32]),
         "kites_selector_save": (c_int, [vp, vp, u32]),
         "kites_graph_set_tpv": (c_int, [vp, c_int]),
+        "kites_sssp_multi_seed": (c_int, [vp, vp, c_int, vp, u64, vp, POINTER(RunOpts),
+                                          POINTER(RunStats)]),
+        "kites_gen_rmat_union": (c_int, [u32, u64, u32, u32, u32, u32, u32, u32, vp, vp, vp,
+                                         vp, vp]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)
@@ -366,6 +371,17 @@ class Graph:
                                        ctypes.byref(o), ctypes.byref(st)))
         return out, st
 
+    def sssp_multi_seed(self, seeds, op=OP_SSSP, out=None, opts=None):
+        st = RunStats()
+        o = opts or default_opts()
+        sd = np.ascontiguousarray(seeds, dtype=np.uint32)
+        if out is None:
+            out = np.empty(self.n_vertices, dtype=np.uint32)
+        ptr = None if out is False else _p(out)
+        _check(load().kites_sssp_multi_seed(self.engine._h, self._h, op, _p(sd), sd.shape[0],
+                                            ptr, ctypes.byref(o), ctypes.byref(st)))
+        return (None if out is False else out), st
+
     def selector_record(self, op=OP_SSSP, source=0, capacity=512):
         """Per iteration: 12 features and the time (ms) of each selector class."""
         X = np.zeros((capacity, SELECTOR_FEATURES), dtype=np.float32)
@@ -412,6 +428,24 @@ def gen_rmat(scale, n_edges, a=0.57, b=0.19, c=0.19, seed=1, w_lo=1, w_hi=255,
     _check(load().kites_gen_rmat(scale, n_vertices, n_edges, a, b, c, seed, w_lo, w_hi,
                                  _p(src), _p(dst), _p(w)))
     return src, dst, w
+
+
+def gen_rmat_union(n_graphs, seed=1, v_min=1000, v_max=100000, ef_min=4, ef_max=32, w_lo=1,
+                   w_hi=255):
+    """Disjoint union of R-MAT graphs; returns (src, dst, w, vertex_offsets,
+    edge_offsets) with global vertex ids."""
+    vo = np.zeros(n_graphs + 1, dtype=np.uint64)
+    eo = np.zeros(n_graphs + 1, dtype=np.uint64)
+    lib = load()
+    _check(lib.kites_gen_rmat_union(n_graphs, seed, v_min, v_max, ef_min, ef_max, w_lo, w_hi,
+                                    _p(vo), _p(eo), None, None, None))
+    m = int(eo[-1])
+    src = np.empty(m, dtype=np.uint32)
+    dst = np.empty(m, dtype=np.uint32)
+    w = np.empty(m, dtype=np.uint32)
+    _check(lib.kites_gen_rmat_union(n_graphs, seed, v_min, v_max, ef_min, ef_max, w_lo, w_hi,
+                                    _p(vo), _p(eo), _p(src), _p(dst), _p(w)))
+    return src, dst, w, vo, eo
 
 
 def gen_er(n_vertices, n_edges, seed=1, w_lo=1, w_hi=255):

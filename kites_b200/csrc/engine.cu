@@ -1617,6 +1617,56 @@ extern "C" int kites_sssp_batch(kites_engine *eng, kites_graph *g, int op,
                   : dispatch_batch<uint32_t>(g, op, host_src, k, dist_out, o, stats);
 }
 
+// ---- multi-seed (multi-graph batches) --------------------------------------------
+
+extern "C" int kites_sssp_multi_seed(kites_engine *eng, kites_graph *g, int op,
+                                     const uint32_t *seeds, uint64_t n_seeds,
+                                     uint32_t *dist_out, const kites_run_opts *opts,
+                                     kites_run_stats *stats) {
+  clear_error();
+  KITES_TRY(check_graph(eng, g));
+  if (op != OP_SSSP && op != OP_SSSP_WRAP && op != OP_BFS)
+    return fail(KITES_ERR_INVALID, "multi-seed runs take SSSP, SSSP_WRAP or BFS");
+  if (!seeds || n_seeds == 0) return fail(KITES_ERR_INVALID, "no seeds");
+  std::vector<uint32_t> hs(n_seeds);
+  KITES_CUDA_TRY(cudaMemcpy(hs.data(), seeds, n_seeds * 4, cudaMemcpyDefault));
+  for (uint64_t i = 0; i < n_seeds; ++i)
+    if (hs[i] >= g->n_given) return fail(KITES_ERR_INVALID, "seed %u out of range", hs[i]);
+  cudaStream_t s = eng->stream;
+  auto t0 = std::chrono::steady_clock::now();
+  void *p;
+  KITES_TRY(dev_alloc(eng, &p, n_seeds * 4));
+  uint32_t *dseeds = (uint32_t *)p;
+  KITES_CUDA_TRY(cudaMemcpyAsync(dseeds, hs.data(), n_seeds * 4, cudaMemcpyHostToDevice, s));
+  k_fill_u32<<<grid_for(g->n), 256, 0, s>>>((uint32_t *)g->V, g->n, kInf);
+  KITES_CUDA_TRY(cudaMemsetAsync(g->bitmaps, 0, 4 * g->nwords * 4, s));
+  const bool strategies = opts && opts->strategy != KITES_STRATEGY_PLAIN;
+  const unsigned blocks = (unsigned)std::min<uint64_t>(n_seeds, 65535);
+  if (g->off64)
+    k_seed_many<uint64_t><<<blocks, 128, 0, s>>>((uint32_t *)g->V, dseeds, n_seeds,
+                                                 (const uint64_t *)g->outR, g->outC, g->shift,
+                                                 strategies ? g->changed[0] : g->frontier[0],
+                                                 strategies ? 1 : 0);
+  else
+    k_seed_many<uint32_t><<<blocks, 128, 0, s>>>((uint32_t *)g->V, dseeds, n_seeds,
+                                                 (const uint32_t *)g->outR, g->outC, g->shift,
+                                                 strategies ? g->changed[0] : g->frontier[0],
+                                                 strategies ? 1 : 0);
+  KITES_CUDA_TRY(cudaGetLastError());
+  KITES_CUDA_TRY(cudaFreeAsync(dseeds, s));
+  int st = strategies ? run_strategies(eng, g, op, opts, stats)
+                      : kites_process(eng, g, op, opts, stats);
+  if (st != KITES_OK) return st;
+  if (dist_out) {
+    KITES_CUDA_TRY(cudaMemcpyAsync(dist_out, g->V, g->n_given * 4, cudaMemcpyDefault, s));
+    KITES_CUDA_TRY(cudaStreamSynchronize(s));
+  }
+  if (stats)
+    stats->host_ms = std::chrono::duration<double, std::milli>(
+                         std::chrono::steady_clock::now() - t0).count();
+  return KITES_OK;
+}
+
 // ---- learned selector ------------------------------------------------------------
 
 extern "C" int kites_selector_record(kites_engine *eng, kites_graph *g, int op, uint32_t source,

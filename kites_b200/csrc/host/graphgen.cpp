@@ -30,14 +30,17 @@ void radix_sort(std::vector<rec> &a, uint32_t bits) {
   const size_t n = a.size();
   if (n < 2 || bits == 0) return;
   std::vector<rec> b(n);
-  int nthreads = omp_get_max_threads();
-  std::vector<size_t> hist(kBuckets * nthreads);
+  // Partition by the size of the team actually running (1 when called from
+  // inside another parallel region).
+  const int max_threads = omp_get_max_threads();
+  std::vector<size_t> hist(kBuckets * max_threads);
   rec *src = a.data(), *dst = b.data();
   int passes = 0;
   for (uint32_t shift = 0; shift < bits; shift += kDigit, ++passes) {
     std::fill(hist.begin(), hist.end(), 0);
-#pragma omp parallel num_threads(nthreads)
+#pragma omp parallel num_threads(max_threads)
     {
+      const int nthreads = omp_get_num_threads();
       int t = omp_get_thread_num();
       size_t lo = n * t / nthreads, hi = n * (t + 1) / nthreads;
       size_t *h = &hist[kBuckets * t];
@@ -107,10 +110,11 @@ int dedup_topup(uint64_t n_edges, uint32_t key_bits, CandFn cand,
       continue;
     }
     // Ordered compaction of the first n_edges kept candidates.
-    int nthreads = omp_get_max_threads();
-    std::vector<uint64_t> counts(nthreads + 1, 0);
-#pragma omp parallel num_threads(nthreads)
+    const int max_threads = omp_get_max_threads();
+    std::vector<uint64_t> counts(max_threads + 1, 0);
+#pragma omp parallel num_threads(max_threads)
     {
+      const int nthreads = omp_get_num_threads();
       int t = omp_get_thread_num();
       uint64_t lo = N * t / nthreads, hi = N * (t + 1) / nthreads, c = 0;
       for (uint64_t i = lo; i < hi; ++i) c += keep[i];
@@ -255,5 +259,55 @@ extern "C" int kites_csc_from_edges(uint64_t n_vertices, uint64_t n_edges,
     C[i] = (uint32_t)(r[i].key & 0xFFFFFFFFu);
     if (E) E[i] = r[i].val;
   }
+  return KITES_OK;
+}
+
+// Disjoint union of n_graphs R-MAT graphs (a,b,c = 0.57,0.19,0.19): graph i
+// has V_i log-uniform in [v_min, v_max] and edge factor uniform in
+// [ef_min, ef_max] (one SplitMix64 stream per graph for the sizes, seed
+// seed * 1000003 + i for its edges); vertex ids of graph i are shifted by
+// vertex_offsets[i].  With src == NULL only the offsets are computed.
+extern "C" int kites_gen_rmat_union(uint32_t n_graphs, uint64_t seed, uint32_t v_min,
+                                    uint32_t v_max, uint32_t ef_min, uint32_t ef_max,
+                                    uint32_t w_lo, uint32_t w_hi, uint64_t *vertex_offsets,
+                                    uint64_t *edge_offsets, uint32_t *src, uint32_t *dst,
+                                    uint32_t *w) {
+  kites_internal::clear_error();
+  if (!n_graphs || v_min < 2 || v_max < v_min || ef_max < ef_min || !ef_min ||
+      !vertex_offsets || !edge_offsets || w_lo > w_hi)
+    return kites_internal::fail(KITES_ERR_INVALID, "bad union arguments");
+  const uint64_t base = kites_gen::stream_base(seed ^ 0x5eed5eedull);
+  vertex_offsets[0] = edge_offsets[0] = 0;
+  std::vector<uint32_t> nv(n_graphs), ef(n_graphs);
+  for (uint32_t i = 0; i < n_graphs; ++i) {
+    const double u = (double)(kites_gen::draw(base, i, 0) >> 11) * (1.0 / 9007199254740992.0);
+    const double lv = std::log((double)v_min) + u * (std::log((double)v_max) - std::log((double)v_min));
+    nv[i] = std::min<uint32_t>(v_max, std::max<uint32_t>(v_min, (uint32_t)std::floor(std::exp(lv))));
+    ef[i] = kites_gen::uniform_u32(kites_gen::draw(base, i, 1), ef_min, ef_max);
+    vertex_offsets[i + 1] = vertex_offsets[i] + nv[i];
+    edge_offsets[i + 1] = edge_offsets[i] + (uint64_t)nv[i] * ef[i];
+  }
+  if (vertex_offsets[n_graphs] > 0xFFFFFF00ull)
+    return kites_internal::fail(KITES_ERR_INVALID, "union exceeds 32-bit vertex ids");
+  if (!src) return KITES_OK;
+  if (!dst) return kites_internal::fail(KITES_ERR_INVALID, "null dst");
+  int bad = 0;
+#pragma omp parallel for schedule(dynamic, 1) reduction(| : bad)
+  for (int64_t i = 0; i < (int64_t)n_graphs; ++i) {
+    uint32_t scale = 1;
+    while ((1u << scale) < nv[i]) ++scale;
+    const uint64_t eo = edge_offsets[i], m = edge_offsets[i + 1] - eo;
+    if (kites_gen_rmat(scale, nv[i], m, 0.57, 0.19, 0.19, seed * 1000003ull + (uint64_t)i, w_lo,
+                       w_hi, src + eo, dst + eo, w ? w + eo : nullptr) != KITES_OK) {
+      bad = 1;
+      continue;
+    }
+    const uint32_t vo = (uint32_t)vertex_offsets[i];
+    for (uint64_t e = 0; e < m; ++e) {
+      src[eo + e] += vo;
+      dst[eo + e] += vo;
+    }
+  }
+  if (bad) return kites_internal::fail(KITES_ERR_INVALID, "a union member could not be generated");
   return KITES_OK;
 }

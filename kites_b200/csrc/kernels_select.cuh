@@ -306,6 +306,27 @@ __global__ void k_mlp_neutral(float *P) {
     P[i] = (i >= kOffStd && i < kOffStd + kFeat) ? 1.f : 0.f;
 }
 
+// Seeds at distance 0.  as_changed: each seed's bit in the changed set (the
+// strategy loops); otherwise the frontier bits of every seed's out-neighbour
+// groups (the plain loop, like the example's pre-processing).
+template <typename OffT>
+__global__ void k_seed_many(uint32_t *V, const uint32_t *__restrict__ seeds, uint64_t n_seeds,
+                            const OffT *__restrict__ outR, const uint32_t *__restrict__ outC,
+                            uint32_t shift, uint32_t *bits, int as_changed) {
+  for (uint64_t i = blockIdx.x; i < n_seeds; i += gridDim.x) {
+    const uint32_t s = seeds[i];
+    if (threadIdx.x == 0) {
+      V[s] = 0u;
+      if (as_changed) atomicOr(bits + (s >> 5), 1u << (s & 31u));
+    }
+    if (!as_changed)
+      for (OffT j = outR[s] + threadIdx.x; j < outR[s + 1]; j += blockDim.x) {
+        const uint32_t gbit = outC[j] >> shift;
+        atomicOr(bits + (gbit >> 5), 1u << (gbit & 31u));
+      }
+  }
+}
+
 // Sets V[source] = 0 and the source's bit in the changed set.
 __global__ void k_seed_changed(uint32_t *V, uint32_t source, uint32_t *U) {
   if (threadIdx.x == 0 && blockIdx.x == 0) {
