@@ -55,6 +55,7 @@ struct run_counters {
   unsigned long long queue_len[2];    // compacted changed queue lengths
   unsigned long long last_active;     // active / edges of the previous iteration
   unsigned long long last_edges;
+  unsigned long long last_out_edges;  // activation edges of the previous iteration
   uint32_t sel;                       // strategy class picked for the next iteration
   uint32_t pad1;
 };

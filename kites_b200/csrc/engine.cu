@@ -17,6 +17,7 @@
 #include "kernels_pr.cuh"
 #include "kernels_select.cuh"
 #include "kernels_strategy.cuh"
+#include "kernels_sweep.cuh"
 
 using namespace kites_internal;
 
@@ -31,8 +32,10 @@ namespace {
 
 int dev_alloc(kites_engine *eng, void **p, size_t bytes) {
   *p = nullptr;
-  if (bytes == 0) bytes = 256;
-  bytes = (bytes + 255) & ~size_t(255);
+  // At least 16 bytes of slack past the end: the staged sweep copies whole
+  // 16-byte pieces, so a slice ending inside the last piece reads up to 12
+  // bytes beyond the array.
+  bytes = (bytes + 16 + 255) & ~size_t(255);
   cudaError_t e = cudaMallocFromPoolAsync(p, bytes, eng->pool, eng->stream);
   if (e != cudaSuccess) {
     cudaGetLastError();
@@ -116,6 +119,29 @@ int upload_offsets(kites_graph *g, const uint64_t *src64, const uint32_t *src32,
     KITES_CUDA_TRY(cudaGetLastError());
   }
   *out = R;
+  return KITES_OK;
+}
+
+// Every instantiation of the staged sweep needs more than the default 48 KB
+// of dynamic shared memory.
+template <typename OffT>
+int init_sweep_attrs() {
+  static bool done = false;
+  if (done) return KITES_OK;
+  const int bytes = (int)sweep_smem_bytes<OffT>();
+#define KITES_SWEEP_ATTR(OPV, MODE)                                                        \
+  KITES_CUDA_TRY(cudaFuncSetAttribute(k_sweep<OPV, OffT, MODE>,                            \
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, bytes))
+  KITES_SWEEP_ATTR(OP_SSSP, kRowFilter);
+  KITES_SWEEP_ATTR(OP_SSSP_WRAP, kRowFilter);
+  KITES_SWEEP_ATTR(OP_BFS, kRowFilter);
+  KITES_SWEEP_ATTR(OP_CC, kRowFilter);
+  KITES_SWEEP_ATTR(OP_SSSP, kEdgeFilter);
+  KITES_SWEEP_ATTR(OP_SSSP_WRAP, kEdgeFilter);
+  KITES_SWEEP_ATTR(OP_BFS, kEdgeFilter);
+  KITES_SWEEP_ATTR(OP_CC, kEdgeFilter);
+#undef KITES_SWEEP_ATTR
+  done = true;
   return KITES_OK;
 }
 
@@ -294,10 +320,38 @@ int upload_typed(kites_graph *g, const kites_csc_view *v) {
   g->pull_grid = (int)(want < cap ? (want ? want : 1) : cap);
   want = (g->nchunks_dir + kWarpsPerBlock - 1) / kWarpsPerBlock;
   g->expand_grid = (int)(want < cap ? (want ? want : 1) : cap);
+
+  // Staged sweep: tile table, shared-memory opt-in, persistent grid.
+  if (g->vpg == 1) {
+    KITES_TRY(init_sweep_attrs<OffT>());
+    const uint32_t saved = g->chunk_items;
+    g->chunk_items = kTileItems;
+    const int st = build_chunk_table<OffT>(g, (const OffT *)g->R, g->n, g->m, &g->chunk_tile,
+                                           &g->ntiles);
+    g->chunk_items = saved;
+    KITES_TRY(st);
+    int per_sm_sweep = 0;
+    KITES_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &per_sm_sweep, k_sweep<OP_SSSP, OffT, kRowFilter>, kSweepThreads,
+        sweep_smem_bytes<OffT>()));
+    const uint64_t scap = (uint64_t)std::max(per_sm_sweep, 1) * eng->sm_count;
+    g->sweep_grid = (int)std::max<uint64_t>(1, std::min<uint64_t>(g->ntiles, scap));
+    g->dense_edges = g->m / 16;
+  }
   return KITES_OK;
 }
 
 // ---- iteration loops ----------------------------------------------------
+
+template <int OP, typename OffT, int MODE>
+void launch_sweep(kites_graph *g, const uint32_t *rd, const uint32_t *U, uint32_t *chg,
+                  uint32_t gate, uint32_t gate_cur) {
+  sweep_args<OffT> a{(const OffT *)g->R, g->C, (const uint32_t *)g->E, (uint32_t *)g->V,
+                     g->chunk_tile, g->ntiles, g->n, g->n + g->m, rd, U, chg, g->ctr, g->m,
+                     gate, gate_cur, g->dense_edges};
+  k_sweep<OP, OffT, MODE><<<g->sweep_grid, kSweepThreads, sweep_smem_bytes<OffT>(),
+                            g->eng->stream>>>(a);
+}
 
 // One iteration of the plain strategy: pull, activation, clear, check.
 template <int OP, typename OffT>
@@ -307,9 +361,19 @@ int launch_iteration(kites_graph *g, int parity, cudaGraphConditionalHandle h,
   if (time_pull) KITES_CUDA_TRY(cudaEventRecord(g->eng->kev0, s));
   chunk_geom<OffT> gin{(const OffT *)g->R, g->C, g->chunk_in, g->nchunks_in,
                        g->n, g->n + g->m, g->chunk_items};
+  // Sparse frontiers: per-row chunked pull; dense ones (activation edges of
+  // the previous iteration above dense_edges): the staged sweep.  Both are
+  // launched, the gate lets exactly one do the work.
+  const bool sweep = g->chunk_tile != nullptr;
   pull_args<OffT> pa{gin, (const uint32_t *)g->E, (uint32_t *)g->V,
-                     g->frontier[parity], g->changed[parity], g->shift, g->ctr};
+                     g->frontier[parity], g->changed[parity], g->shift, g->ctr, nullptr,
+                     sweep ? 1u : 0u, 0u, g->dense_edges};
   k_pull_chunked<OP, OffT><<<g->pull_grid, kBlock, 0, s>>>(pa);
+  if (sweep) {
+    launch_sweep<OP, OffT, kRowFilter>(g, g->frontier[parity], nullptr, g->changed[parity],
+                                       2u, 0u);
+    ++*launches;
+  }
   if (time_pull) KITES_CUDA_TRY(cudaEventRecord(g->eng->kev1, s));
   chunk_geom<OffT> gdir{(const OffT *)g->dirR, g->dirC, g->chunk_dir, g->nchunks_dir,
                         g->n_dir_rows, g->n_dir_rows + g->n_dir_edges, g->chunk_items};
@@ -604,8 +668,12 @@ int launch_strategy(kites_graph *g, const flex_state &f, int strategy, int parit
   switch (strategy) {
     case KITES_STRATEGY_PLAIN: {
       expand();
-      pull_args<OffT> pa{gin, (const uint32_t *)g->E, (uint32_t *)g->V, f.A, Unext, 0, g->ctr};
+      // The expansion just counted this iteration's activation edges.
+      pull_args<OffT> pa{gin, (const uint32_t *)g->E, (uint32_t *)g->V, f.A, Unext, 0, g->ctr,
+                         nullptr, 1u, 1u, g->dense_edges};
       k_pull_chunked<OP, OffT><<<g->pull_grid, kBlock, 0, s>>>(pa);
+      launch_sweep<OP, OffT, kRowFilter>(g, f.A, nullptr, Unext, 2u, 1u);
+      ++*launches;
       break;
     }
     case KITES_STRATEGY_PUSH: {
@@ -617,9 +685,7 @@ int launch_strategy(kites_graph *g, const flex_state &f, int strategy, int parit
       break;
     }
     case KITES_STRATEGY_PULL_ALL: {
-      pull_args<OffT> pa{gin, (const uint32_t *)g->E, (uint32_t *)g->V, nullptr, Unext, 0,
-                         g->ctr, Ucur};
-      k_pull_all<OP, OffT><<<g->pull_grid, kBlock, 0, s>>>(pa);
+      launch_sweep<OP, OffT, kEdgeFilter>(g, nullptr, Ucur, Unext, 0u, 0u);
       break;
     }
     case KITES_STRATEGY_TPV1:

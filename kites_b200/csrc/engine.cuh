@@ -66,6 +66,12 @@ struct kites_graph {
   uint32_t *chunk_dir = nullptr;
   uint64_t nchunks_dir = 0;
 
+  // Tiles of the staged dense sweep (kTileItems items each), vpg == 1 only.
+  uint32_t *chunk_tile = nullptr;
+  uint64_t ntiles = 0;
+  int sweep_grid = 0;
+  unsigned long long dense_edges = 0;   // PLAIN switches to the sweep above this
+
   // Frontier: [f0 | c0 | f1 | c1], nwords each.
   uint32_t *bitmaps = nullptr;
   uint64_t nbits = 0, nwords = 0;

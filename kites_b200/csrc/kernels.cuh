@@ -151,7 +151,17 @@ struct pull_args {
   uint32_t shift;          // log2(vertex_per_group)
   run_counters *ctr;
   const uint32_t *U;       // filtered pull: changed set of the previous iteration
+  // Density gate: 0 always run; 1 run only while the frontier is sparse (the
+  // staged sweep takes dense frontiers).  Dense = activation edges (this
+  // iteration's when gate_cur, else the previous one's) above dense_edges.
+  uint32_t gate, gate_cur;
+  unsigned long long dense_edges;
 };
+
+__device__ __forceinline__ bool frontier_dense(const run_counters *c, uint32_t cur,
+                                               unsigned long long dense_edges) {
+  return (cur ? c->out_edges : c->last_out_edges) > dense_edges;
+}
 
 // The pull iteration over the edge-balanced chunks.  Rows whose frontier
 // bit is set (every row when rd is null) fold their in-edges with the edge
@@ -243,6 +253,7 @@ __device__ __forceinline__ void pull_chunks(const pull_args<OffT> &a) {
 template <int OP, typename OffT>
 __global__ void __launch_bounds__(kBlock) k_pull_chunked(pull_args<OffT> a) {
   if (a.ctr->done) return;
+  if (a.gate == 1 && frontier_dense(a.ctr, a.gate_cur, a.dense_edges)) return;
   pull_chunks<OP, OffT, false>(a);
 }
 
@@ -356,6 +367,7 @@ __global__ void k_loop_check(run_counters *c, iter_record rec,
   c->iterations = it + 1;
   c->last_active = c->active;
   c->last_edges = c->edges;
+  c->last_out_edges = c->out_edges;
   c->queue_len[0] = 0;
   c->total_active += c->active;
   c->total_edges += c->edges;
