@@ -257,6 +257,31 @@ int kites_selector_save(kites_engine *eng, float *params, uint32_t n_params);
  * (KITES_STRATEGY_TPV1/4/8/32). */
 int kites_graph_set_tpv(kites_graph *g, int strategy);
 
+/* ---- autotuner ---------------------------------------------------------
+ * No reference counterpart (the reference fixes 128 threads per block and
+ * one vertex per thread).  Times candidate tile shapes on this graph with
+ * the given sources and keeps the fastest: the batched kernel's chunk size
+ * (vertices + edges per warp), the threads-per-vertex width of the
+ * selector's TPV class, and the frontier densities at which the plain loop
+ * switches its pull and its activation to the staged sweeps. */
+typedef struct kites_tune_result {
+  uint32_t batch_chunk_items;
+  int32_t tpv_strategy;
+  uint64_t dense_edges;
+  uint64_t dense_rows;
+  float batch_ms;          /* best batched run time             */
+  float plain_ms;          /* best plain single-source run time */
+  float tpv_ms;            /* best TPV single-source run time   */
+  uint32_t trials;
+} kites_tune_result;
+
+int kites_autotune(kites_engine *eng, kites_graph *g, int op, const uint32_t *sources,
+                   uint32_t n_sources, uint32_t batch, kites_tune_result *out);
+/* Sets the two densities by hand: the plain loop's pull uses the staged sweep
+ * when the activation edges exceed dense_edges, its activation when the
+ * changed rows exceed dense_rows (0 = always, UINT64_MAX = never). */
+int kites_graph_set_density(kites_graph *g, uint64_t dense_edges, uint64_t dense_rows);
+
 /* ---- synthetic graphs (host, deterministic, OpenMP) ------------------ */
 
 /* Candidate edges come from a counter-based SplitMix64 stream; self-loops,

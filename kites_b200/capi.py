@@ -36,7 +36,8 @@ EXPORTED = [
     "kites_cc", "kites_pagerank", "kites_gen_rmat", "kites_gen_er", "kites_gen_grid",
     "kites_csc_from_edges", "kites_selector_record", "kites_selector_train",
     "kites_selector_load", "kites_selector_save", "kites_graph_set_tpv",
-    "kites_sssp_multi_seed", "kites_gen_rmat_union",
+    "kites_sssp_multi_seed", "kites_gen_rmat_union", "kites_autotune",
+    "kites_graph_set_density",
 ]
 SELECTOR_FEATURES, SELECTOR_CLASSES, SELECTOR_PARAMS = 12, 4, 1628
 # Parameter layout of the selector MLP (offsets into the 1628 floats).
@@ -91,6 +92,14 @@ class RunStats(Structure):
         ("iter_ms", c_float * MAX_RECORDED_ITERS),
         ("iter_active", c_uint64 * MAX_RECORDED_ITERS),
         ("iter_edges", c_uint64 * MAX_RECORDED_ITERS),
+    ]
+
+
+class TuneResult(Structure):
+    _fields_ = [
+        ("batch_chunk_items", c_uint32), ("tpv_strategy", c_int32),
+        ("dense_edges", c_uint64), ("dense_rows", c_uint64), ("batch_ms", c_float),
+        ("plain_ms", c_float), ("tpv_ms", c_float), ("trials", c_uint32),
     ]
 
 
@@ -150,6 +159,8 @@ def load(path: str = LIB_PATH):
                                           POINTER(RunStats)]),
         "kites_gen_rmat_union": (c_int, [u32, u64, u32, u32, u32, u32, u32, u32, vp, vp, vp,
                                          vp, vp]),
+        "kites_autotune": (c_int, [vp, vp, c_int, vp, u32, u32, POINTER(TuneResult)]),
+        "kites_graph_set_density": (c_int, [vp, u64, u64]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)
@@ -393,6 +404,13 @@ class Graph:
 
     def set_tpv(self, strategy):
         _check(load().kites_graph_set_tpv(self._h, strategy))
+
+    def autotune(self, sources, batch=64, op=OP_SSSP):
+        src = np.ascontiguousarray(sources, dtype=np.uint32)
+        r = TuneResult()
+        _check(load().kites_autotune(self.engine._h, self._h, op, _p(src), src.shape[0], batch,
+                                     ctypes.byref(r)))
+        return r
 
     def cc(self, out=None, opts=None):
         st = RunStats()

@@ -56,6 +56,8 @@ struct run_counters {
   unsigned long long last_active;     // active / edges of the previous iteration
   unsigned long long last_edges;
   unsigned long long last_out_edges;  // activation edges of the previous iteration
+  unsigned long long changed;         // rows marked changed by the pull/push kernels
+  unsigned long long last_changed;
   uint32_t sel;                       // strategy class picked for the next iteration
   uint32_t pad1;
 };

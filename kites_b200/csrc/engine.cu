@@ -141,6 +141,8 @@ int init_sweep_attrs() {
   KITES_SWEEP_ATTR(OP_BFS, kEdgeFilter);
   KITES_SWEEP_ATTR(OP_CC, kEdgeFilter);
 #undef KITES_SWEEP_ATTR
+  KITES_CUDA_TRY(cudaFuncSetAttribute(k_expand_sweep<OffT>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
   done = true;
   return KITES_OK;
 }
@@ -337,6 +339,20 @@ int upload_typed(kites_graph *g, const kites_csc_view *v) {
     const uint64_t scap = (uint64_t)std::max(per_sm_sweep, 1) * eng->sm_count;
     g->sweep_grid = (int)std::max<uint64_t>(1, std::min<uint64_t>(g->ntiles, scap));
     g->dense_edges = g->m / 16;
+    // Tiles of the activation adjacency (the in-CSC itself when undirected).
+    if (g->dirR == g->R) {
+      g->chunk_tile_dir = g->chunk_tile;
+      g->ntiles_dir = g->ntiles;
+    } else {
+      g->chunk_items = kTileItems;
+      const int st2 = build_chunk_table<OffT>(g, (const OffT *)g->dirR, g->n_dir_rows,
+                                              g->n_dir_edges, &g->chunk_tile_dir,
+                                              &g->ntiles_dir);
+      g->chunk_items = saved;
+      KITES_TRY(st2);
+    }
+    g->expand_sweep_grid = (int)std::max<uint64_t>(1, std::min<uint64_t>(g->ntiles_dir, scap));
+    g->dense_rows = g->n / 32;
   }
   return KITES_OK;
 }
@@ -351,6 +367,29 @@ void launch_sweep(kites_graph *g, const uint32_t *rd, const uint32_t *U, uint32_
                      gate, gate_cur, g->dense_edges};
   k_sweep<OP, OffT, MODE><<<g->sweep_grid, kSweepThreads, sweep_smem_bytes<OffT>(),
                             g->eng->stream>>>(a);
+}
+
+// Activation of the changed rows `chg` into `wr` over an adjacency (rows,
+// targets, chunk and tile tables): the chunked kernel for sparse changed
+// sets, the staged sweep for dense ones (tiles given), one of them working.
+template <typename OffT>
+void launch_expand(kites_graph *g, const void *aR, const uint32_t *aC, const uint32_t *chunks,
+                   uint64_t nchunks, const uint32_t *tiles, uint64_t ntiles, uint64_t rows,
+                   uint64_t edges, const uint32_t *chg, uint32_t *wr, uint32_t gate_cur,
+                   uint64_t *launches) {
+  cudaStream_t s = g->eng->stream;
+  const bool sweep = tiles != nullptr;
+  chunk_geom<OffT> ga{(const OffT *)aR, aC, chunks, nchunks, rows, rows + edges, g->chunk_items};
+  expand_args<OffT> ea{ga, chg, wr, g->ctr, sweep ? 1u : 0u, gate_cur, g->dense_rows};
+  k_expand_chunked<OffT><<<g->expand_grid, kBlock, 0, s>>>(ea);
+  ++*launches;
+  if (sweep) {
+    sweep_args<OffT> sa{(const OffT *)aR, aC, nullptr, nullptr, tiles, ntiles, rows,
+                        rows + edges, chg, nullptr, wr, g->ctr, edges, 2u, gate_cur,
+                        g->dense_rows};
+    k_expand_sweep<OffT><<<g->expand_sweep_grid, kSweepThreads, sweep_smem_bytes<OffT>(), s>>>(sa);
+    ++*launches;
+  }
 }
 
 // One iteration of the plain strategy: pull, activation, clear, check.
@@ -375,17 +414,16 @@ int launch_iteration(kites_graph *g, int parity, cudaGraphConditionalHandle h,
     ++*launches;
   }
   if (time_pull) KITES_CUDA_TRY(cudaEventRecord(g->eng->kev1, s));
-  chunk_geom<OffT> gdir{(const OffT *)g->dirR, g->dirC, g->chunk_dir, g->nchunks_dir,
-                        g->n_dir_rows, g->n_dir_rows + g->n_dir_edges, g->chunk_items};
-  expand_args<OffT> ea{gdir, g->changed[parity], g->frontier[parity ^ 1], g->ctr};
-  k_expand_chunked<OffT><<<g->expand_grid, kBlock, 0, s>>>(ea);
+  launch_expand<OffT>(g, g->dirR, g->dirC, g->chunk_dir, g->nchunks_dir, g->chunk_tile_dir,
+                      g->ntiles_dir, g->n_dir_rows, g->n_dir_edges, g->changed[parity],
+                      g->frontier[parity ^ 1], 1u, launches);
   // Clear the read frontier and the changed bitmap (adjacent words).
   k_clear_words<<<grid_for(2 * g->nwords, 256, 4096), 256, 0, s>>>(g->frontier[parity],
                                                                     2 * g->nwords);
   iter_record rec{g->rec_active, g->rec_edges, KITES_MAX_RECORDED_ITERS};
   k_loop_check<<<1, 1, 0, s>>>(g->ctr, rec, h, has_handle);
   KITES_CUDA_TRY(cudaGetLastError());
-  *launches += 4;
+  *launches += 3;
   return KITES_OK;
 }
 
@@ -399,6 +437,8 @@ struct batch_state {
   const uint32_t *actC;
   const uint32_t *act_chunks;
   uint64_t act_nchunks, act_rows, act_edges;
+  const uint32_t *act_tiles;   // staged-sweep tiles of the adjacency, or null
+  uint64_t act_ntiles;
   int grid;
 };
 
@@ -416,15 +456,13 @@ int launch_batch_iteration(kites_graph *g, const batch_state &b, int parity,
   pull_batch_args<OffT> pa{gb, (const uint32_t *)g->E, b.D, rd, chg, g->ctr};
   k_pull_batch<OP, OffT, K><<<b.grid, kBlock, 0, s>>>(pa);
   if (time_pull) KITES_CUDA_TRY(cudaEventRecord(g->eng->kev1, s));
-  chunk_geom<OffT> ga{(const OffT *)b.actR, b.actC, b.act_chunks, b.act_nchunks, b.act_rows,
-                      b.act_rows + b.act_edges, g->chunk_items};
-  expand_args<OffT> ea{ga, chg, wr, g->ctr};
-  k_expand_chunked<OffT><<<g->expand_grid, kBlock, 0, s>>>(ea);
+  launch_expand<OffT>(g, b.actR, b.actC, b.act_chunks, b.act_nchunks, b.act_tiles,
+                      b.act_ntiles, b.act_rows, b.act_edges, chg, wr, 1u, launches);
   k_clear_words<<<grid_for(2 * b.nwords, 256, 4096), 256, 0, s>>>(rd, 2 * b.nwords);
   iter_record rec{g->rec_active, g->rec_edges, KITES_MAX_RECORDED_ITERS};
   k_loop_check<<<1, 1, 0, s>>>(g->ctr, rec, h, has_handle);
   KITES_CUDA_TRY(cudaGetLastError());
-  *launches += 4;
+  *launches += 3;
   return KITES_OK;
 }
 
@@ -661,9 +699,9 @@ int launch_strategy(kites_graph *g, const flex_state &f, int strategy, int parit
                         g->n_dir_rows, g->n_dir_rows + g->n_dir_edges, g->chunk_items};
   const uint64_t nw = g->nwords;
   auto expand = [&]() {
-    expand_args<OffT> ea{gdir, Ucur, f.A, g->ctr};
-    k_expand_chunked<OffT><<<g->expand_grid, kBlock, 0, s>>>(ea);
-    ++*launches;
+    // U was marked by the previous iteration: its count is last_changed.
+    launch_expand<OffT>(g, g->dirR, g->dirC, g->chunk_dir, g->nchunks_dir, g->chunk_tile_dir,
+                        g->ntiles_dir, g->n_dir_rows, g->n_dir_edges, Ucur, f.A, 0u, launches);
   };
   switch (strategy) {
     case KITES_STRATEGY_PLAIN: {
@@ -1140,12 +1178,16 @@ int prepare_batch(kites_graph *g, uint32_t K, uint32_t items, batch_state *b) {
     b->nwords = g->bnwords;
   }
   // Vertex-level activation adjacency.
+  b->act_tiles = nullptr;
+  b->act_ntiles = 0;
   if (!g->directed) {
     b->actR = g->R; b->actC = g->C; b->act_chunks = g->chunk_in;
     b->act_nchunks = g->nchunks_in; b->act_rows = g->n; b->act_edges = g->m;
+    b->act_tiles = g->chunk_tile; b->act_ntiles = g->ntiles;
   } else if (g->vpg == 1) {
     b->actR = g->dirR; b->actC = g->dirC; b->act_chunks = g->chunk_dir;
     b->act_nchunks = g->nchunks_dir; b->act_rows = g->n; b->act_edges = g->m;
+    b->act_tiles = g->chunk_tile_dir; b->act_ntiles = g->ntiles_dir;
   } else {
     if (!g->chunk_out)
       KITES_TRY(build_chunk_table<OffT>(g, (const OffT *)g->outR, g->n, g->m, &g->chunk_out,
@@ -1164,7 +1206,7 @@ int run_batch(kites_graph *g, const uint32_t *sources, uint32_t *dist_out,
   cudaStream_t s = eng->stream;
   auto t0 = std::chrono::steady_clock::now();
   batch_state b{};
-  const uint32_t items = g->batch_chunk_items ? g->batch_chunk_items : 256u;
+  const uint32_t items = g->batch_items_req ? g->batch_items_req : 256u;
   KITES_TRY(prepare_batch<OffT>(g, K, items, &b));
   int per_sm = 0;
   KITES_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
@@ -1845,5 +1887,120 @@ extern "C" int kites_graph_set_tpv(kites_graph *g, int strategy) {
     }
     g->tpv_strategy = strategy;
   }
+  return KITES_OK;
+}
+
+// ---- autotuner ------------------------------------------------------------------
+
+namespace {
+
+void drop_all_loops(kites_graph *g) {
+  for (auto &kv : g->loops) {
+    cudaGraphExecDestroy(kv.second.second);
+    cudaGraphDestroy(kv.second.first);
+  }
+  g->loops.clear();
+}
+
+}  // namespace
+
+extern "C" int kites_autotune(kites_engine *eng, kites_graph *g, int op, const uint32_t *sources,
+                              uint32_t n_sources, uint32_t batch, kites_tune_result *out) {
+  clear_error();
+  KITES_TRY(check_graph(eng, g));
+  if (!sources || n_sources == 0 || !out) return fail(KITES_ERR_INVALID, "bad arguments");
+  if (op != OP_SSSP && op != OP_BFS) return fail(KITES_ERR_INVALID, "tuning takes SSSP or BFS");
+  memset(out, 0, sizeof(*out));
+  std::vector<uint32_t> src(n_sources);
+  KITES_CUDA_TRY(cudaMemcpy(src.data(), sources, n_sources * 4, cudaMemcpyDefault));
+  kites_run_opts o;
+  kites_default_run_opts(&o);
+  kites_run_stats st;
+  // Runs each source once (the first run of a shape also warms its loop).
+  auto time_single = [&](int strategy, float *ms) -> int {
+    o.strategy = strategy;
+    float total = 0.f;
+    for (uint32_t i = 0; i < std::min<uint32_t>(n_sources, 4); ++i) {
+      KITES_TRY(kites_sssp(eng, g, op, src[i], nullptr, &o, &st));
+      KITES_TRY(kites_sssp(eng, g, op, src[i], nullptr, &o, &st));
+      total += (float)st.device_ms;
+    }
+    *ms = total;
+    ++out->trials;
+    return KITES_OK;
+  };
+  // 1. Density thresholds of the plain loop (vpg == 1 graphs have sweeps).
+  if (g->chunk_tile) {
+    const unsigned long long e_cands[] = {g->m / 64, g->m / 32, g->m / 16, g->m / 8, g->m / 4};
+    const unsigned long long r_cands[] = {g->n / 128, g->n / 64, g->n / 32, g->n / 16, g->n / 8};
+    float best = 1e30f;
+    unsigned long long be = g->dense_edges, br = g->dense_rows;
+    for (unsigned long long e : e_cands) {
+      for (unsigned long long r : r_cands) {
+        g->dense_edges = e;
+        g->dense_rows = r;
+        drop_all_loops(g);
+        float ms;
+        KITES_TRY(time_single(KITES_STRATEGY_PLAIN, &ms));
+        if (ms < best) { best = ms; be = e; br = r; }
+      }
+    }
+    g->dense_edges = be;
+    g->dense_rows = br;
+    out->plain_ms = best;
+  }
+  drop_all_loops(g);
+  out->dense_edges = g->dense_edges;
+  out->dense_rows = g->dense_rows;
+  // 2. Threads per vertex of the selector's TPV class.
+  if (g->vpg == 1 && g->directed) {
+    const int cands[] = {KITES_STRATEGY_TPV1, KITES_STRATEGY_TPV4, KITES_STRATEGY_TPV8,
+                         KITES_STRATEGY_TPV32};
+    float best = 1e30f;
+    int bt = g->tpv_strategy;
+    for (int c : cands) {
+      float ms;
+      KITES_TRY(time_single(c, &ms));
+      if (ms < best) { best = ms; bt = c; }
+    }
+    KITES_TRY(kites_graph_set_tpv(g, bt));
+    out->tpv_ms = best;
+  }
+  out->tpv_strategy = g->tpv_strategy;
+  // 3. Chunk size of the batched kernel.
+  if (batch == 16 || batch == 32 || batch == 64 || batch == 128 || batch == 256) {
+    std::vector<uint32_t> bs(batch);
+    for (uint32_t i = 0; i < batch; ++i) bs[i] = src[i % n_sources];
+    const uint32_t cands[] = {128, 256, 512, 1024, 2048};
+    float best = 1e30f;
+    uint32_t bc = g->batch_chunk_items ? g->batch_chunk_items : 256;
+    kites_run_opts bo;
+    kites_default_run_opts(&bo);
+    for (uint32_t c : cands) {
+      g->batch_items_req = c;  // the next batched run rebuilds its chunk table
+      float total = 0.f;
+      for (int rep = 0; rep < 2; ++rep) {
+        KITES_TRY(kites_sssp_batch(eng, g, op, bs.data(), batch, nullptr, &bo, &st));
+        if (rep) total += (float)st.device_ms;
+      }
+      ++out->trials;
+      if (total < best) { best = total; bc = c; }
+    }
+    g->batch_items_req = bc;
+    out->batch_ms = best;
+  }
+  out->batch_chunk_items = g->batch_items_req ? g->batch_items_req : 256u;
+  return KITES_OK;
+}
+
+extern "C" int kites_graph_set_density(kites_graph *g, uint64_t dense_edges,
+                                       uint64_t dense_rows) {
+  clear_error();
+  if (!g) return fail(KITES_ERR_INVALID, "null graph");
+  KITES_TRY(set_device(g->eng));
+  KITES_CUDA_TRY(cudaStreamSynchronize(g->eng->stream));
+  g->dense_edges = dense_edges;
+  g->dense_rows = dense_rows;
+  drop_all_loops(g);  // captured loops hold the old thresholds
   return KITES_OK;
 }

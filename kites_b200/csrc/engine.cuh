@@ -71,6 +71,10 @@ struct kites_graph {
   uint64_t ntiles = 0;
   int sweep_grid = 0;
   unsigned long long dense_edges = 0;   // PLAIN switches to the sweep above this
+  uint32_t *chunk_tile_dir = nullptr;   // tiles of the activation adjacency
+  uint64_t ntiles_dir = 0;
+  int expand_sweep_grid = 0;
+  unsigned long long dense_rows = 0;    // activation switches to the sweep above this
 
   // Frontier: [f0 | c0 | f1 | c1], nwords each.
   uint32_t *bitmaps = nullptr;
@@ -87,7 +91,8 @@ struct kites_graph {
   uint64_t batch_cap = 0;            // elements of batchD
   uint32_t *bbits = nullptr;         // vertex-level [f0|c0|f1|c1] when vpg > 1
   uint64_t bnwords = 0;
-  uint32_t batch_chunk_items = 0;    // chunk size of chunk_batch (autotuned)
+  uint32_t batch_chunk_items = 0;    // chunk size chunk_batch was built with
+  uint32_t batch_items_req = 0;      // chunk size asked for (autotuner), 0 = 256
   uint32_t *chunk_batch = nullptr;
   uint64_t nchunks_batch = 0;
   uint32_t *chunk_out = nullptr;     // vertex-level out-CSR chunks (vpg > 1)

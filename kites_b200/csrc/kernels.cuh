@@ -176,7 +176,7 @@ __device__ __forceinline__ void pull_chunks(const pull_args<OffT> &a) {
   const uint32_t lane = lane_id(), wib = threadIdx.x >> 5;
   const row_slice<OffT> rs{s_ex[wib], s_lo[wib]};
   uint32_t *acc_s = s_acc[wib];
-  uint32_t n_act = 0, n_edges = 0;
+  uint32_t n_act = 0, n_edges = 0, n_chg = 0;
   const uint64_t stride = (uint64_t)gridDim.x * kWarpsPerBlock;
   for (uint64_t ch = (uint64_t)blockIdx.x * kWarpsPerBlock + wib; ch < a.g.nchunks;
        ch += stride) {
@@ -237,7 +237,8 @@ __device__ __forceinline__ void pull_chunks(const pull_args<OffT> &a) {
       const uint32_t gbit = upd ? (1u << ((v >> a.shift) & 31u)) : 0u;
       const uint32_t bits = __reduce_or_sync(kFull, gbit);
       if (bits && lane == 0) {
-        atomicOr(a.chg + ((vb >> a.shift) >> 5), bits);
+        const uint32_t old = atomicOr(a.chg + ((vb >> a.shift) >> 5), bits);
+        n_chg += __popc(bits & ~old);
         a.ctr->update_flag = 1u;
       }
     }
@@ -247,6 +248,7 @@ __device__ __forceinline__ void pull_chunks(const pull_args<OffT> &a) {
   if (lane == 0) {
     if (n_act) atomicAdd(&a.ctr->active, (unsigned long long)n_act);
     if (n_edges) atomicAdd(&a.ctr->edges, (unsigned long long)n_edges);
+    if (n_chg) atomicAdd(&a.ctr->changed, (unsigned long long)n_chg);
   }
 }
 
@@ -265,13 +267,24 @@ struct expand_args {
   const uint32_t *chg;     // changed rows
   uint32_t *wr;            // write frontier
   run_counters *ctr;
+  // Gate: 0 always run; 1 only while the changed set is sparse (the staged
+  // k_expand_sweep takes dense ones).  Dense = changed rows (this
+  // iteration's when gate_cur, else the previous one's) above dense_rows.
+  uint32_t gate, gate_cur;
+  unsigned long long dense_rows;
 };
+
+__device__ __forceinline__ bool changed_dense(const run_counters *c, uint32_t cur,
+                                              unsigned long long dense_rows) {
+  return (cur ? c->changed : c->last_changed) > dense_rows;
+}
 
 // For each changed row, OR the bit of every target into the write frontier;
 // lanes hitting the same target word in a window combine their bits first.
 template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_expand_chunked(expand_args<OffT> a) {
   if (a.ctr->done) return;
+  if (a.gate == 1 && changed_dense(a.ctr, a.gate_cur, a.dense_rows)) return;
   __shared__ uint32_t s_ex[kWarpsPerBlock][32];
   __shared__ OffT s_lo[kWarpsPerBlock][32];
   const uint32_t lane = lane_id(), wib = threadIdx.x >> 5;
@@ -368,6 +381,8 @@ __global__ void k_loop_check(run_counters *c, iter_record rec,
   c->last_active = c->active;
   c->last_edges = c->edges;
   c->last_out_edges = c->out_edges;
+  c->last_changed = c->changed;
+  c->changed = 0;
   c->queue_len[0] = 0;
   c->total_active += c->active;
   c->total_edges += c->edges;

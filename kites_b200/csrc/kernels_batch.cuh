@@ -69,7 +69,7 @@ __global__ void __launch_bounds__(kBlock)
   using S = batch_shape<K>;
   const uint32_t lane = lane_id(), wib = threadIdx.x >> 5;
   const uint32_t sub = lane / S::LPE, kl = lane % S::LPE;
-  unsigned long long n_act = 0, n_edges = 0;
+  unsigned long long n_act = 0, n_edges = 0, n_chg = 0;
   const uint64_t stride = (uint64_t)gridDim.x * kWarpsPerBlock;
   for (uint64_t ch = (uint64_t)blockIdx.x * kWarpsPerBlock + wib; ch < a.g.nchunks;
        ch += stride) {
@@ -144,7 +144,7 @@ __global__ void __launch_bounds__(kBlock)
         if (__any_sync(kFull, lane_upd)) upd_bits |= 1u << b;
       }
       if (upd_bits && lane == 0) {
-        atomicOr(a.chg + (vb >> 5), upd_bits);
+        n_chg += __popc(upd_bits & ~atomicOr(a.chg + (vb >> 5), upd_bits));
         a.ctr->update_flag = 1u;
       }
     }
@@ -152,6 +152,7 @@ __global__ void __launch_bounds__(kBlock)
   if (lane == 0) {
     if (n_act) atomicAdd(&a.ctr->active, n_act);
     if (n_edges) atomicAdd(&a.ctr->edges, n_edges);
+    if (n_chg) atomicAdd(&a.ctr->changed, n_chg);
   }
 }
 

@@ -216,7 +216,7 @@ __global__ void __launch_bounds__(128)
   const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
   float l = 0.f;
   if (s < n) {
-    float xn[kFeat], z1[kH], h1[kH], z2[kH], h2[kH], o[kClasses];
+    float xn[kFeat], z1[kH], h1[kH], z2[kH], h2[kH];
 #pragma unroll
     for (int i = 0; i < kFeat; ++i)
       xn[i] = (X[(uint64_t)s * kFeat + i] - sp[kOffMean + i]) / sp[kOffStd + i];
@@ -237,7 +237,6 @@ __global__ void __launch_bounds__(128)
     for (int k = 0; k < kClasses; ++k) {
       float a = sp[kOffB3 + k];
       for (int i = 0; i < kH; ++i) a += sp[kOffW3 + k * kH + i] * h2[i];
-      o[k] = a;
       const float e = a - Y[(uint64_t)s * kClasses + k];
       l += e * e;
       d3[k] = 2.f * e / (float)n;
@@ -268,7 +267,6 @@ __global__ void __launch_bounds__(128)
       atomicAdd(&sg[kOffB1 + j], g);
       for (int i = 0; i < kFeat; ++i) atomicAdd(&sg[kOffW1 + j * kFeat + i], g * xn[i]);
     }
-    (void)o;
   }
   for (int d = 16; d; d >>= 1) l += __shfl_xor_sync(kFull, l, d);
   if (lane_id() == 0 && l != 0.f) atomicAdd(loss, l / (float)n);

@@ -77,6 +77,7 @@ __global__ void __launch_bounds__(kBlock) k_push_queue(push_args<OffT> a) {
   const uint32_t lane = lane_id();
   const unsigned long long qn = a.ctr->queue_len[0];
   unsigned long long n_edges = 0;
+  uint32_t n_chg = 0;
   bool any = false;
   for (unsigned long long i = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < qn;
        i += ((uint64_t)gridDim.x * blockDim.x) >> 5) {
@@ -89,14 +90,17 @@ __global__ void __launch_bounds__(kBlock) k_push_queue(push_args<OffT> a) {
       const uint32_t w = op_reads_weights<OP>() ? __ldcs(a.outE + j) : 0u;
       const uint32_t nd = nbr_comp<OP>(du, w);
       if (nd < a.V[v] && nd < atomicMin(a.V + v, nd)) {
-        atomicOr(a.Unext + (v >> 5), 1u << (v & 31u));
+        const uint32_t bit = 1u << (v & 31u);
+        if (!(atomicOr(a.Unext + (v >> 5), bit) & bit)) ++n_chg;
         any = true;
       }
     }
   }
   if (__any_sync(kFull, any) && lane == 0) a.ctr->update_flag = 1u;
+  n_chg = __reduce_add_sync(kFull, n_chg);
   if (lane == 0) {
     if (n_edges) atomicAdd(&a.ctr->edges, n_edges);
+    if (n_chg) atomicAdd(&a.ctr->changed, (unsigned long long)n_chg);
   }
 }
 
@@ -134,7 +138,7 @@ __global__ void __launch_bounds__(kBlock) k_pull_tpv(pull_tpv_args<OffT> a) {
   const uint32_t lane = lane_id();
   const uint32_t grp = lane / TPV, gl = lane % TPV;
   const uint32_t gmask = (TPV == 32) ? kFull : (((1u << TPV) - 1u) << (grp * TPV));
-  unsigned long long n_act = 0, n_edges = 0;
+  unsigned long long n_act = 0, n_edges = 0, n_chg = 0;
   for (uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < a.nwords;
        w += ((uint64_t)gridDim.x * blockDim.x) >> 5) {
     uint32_t mask = a.A[w];
@@ -172,7 +176,7 @@ __global__ void __launch_bounds__(kBlock) k_pull_tpv(pull_tpv_args<OffT> a) {
     }
     upd_bits = __reduce_or_sync(kFull, upd_bits);
     if (upd_bits && lane == 0) {
-      atomicOr(a.Unext + w, upd_bits);
+      n_chg += __popc(upd_bits & ~atomicOr(a.Unext + w, upd_bits));
       a.ctr->update_flag = 1u;
     }
   }
@@ -181,6 +185,7 @@ __global__ void __launch_bounds__(kBlock) k_pull_tpv(pull_tpv_args<OffT> a) {
   if (lane == 0) {
     if (n_act) atomicAdd(&a.ctr->active, n_act);
     if (n_edges) atomicAdd(&a.ctr->edges, n_edges);
+    if (n_chg) atomicAdd(&a.ctr->changed, n_chg);
   }
 }
 

@@ -120,7 +120,7 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(sweep_args<OffT> a) {
   }
   uint32_t *acc_s = base + 2 * (rwords + 2 * kStageWords);  // kTileItems + 1 rows
   const uint32_t tid = threadIdx.x, lane = lane_id();
-  uint32_t n_act = 0, n_edges = 0;
+  uint32_t n_act = 0, n_edges = 0, n_chg = 0;
   const uint64_t stride = gridDim.x;
   uint64_t t = blockIdx.x;
   if (t < a.ntiles) stage_tile<OffT, kW>(a, tile_of(a, t), Rs[0], Cs[0], Es[0]);
@@ -241,8 +241,8 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(sweep_args<OffT> a) {
       const uint32_t bal = __ballot_sync(kFull, bit);
       if (bal && lane == 0) {
         const uint32_t lo = bal << off, hi = off ? (bal >> (32u - off)) : 0u;
-        if (lo) atomicOr(a.chg + w0, lo);
-        if (hi) atomicOr(a.chg + w0 + 1, hi);
+        if (lo) n_chg += __popc(lo & ~atomicOr(a.chg + w0, lo));
+        if (hi) n_chg += __popc(hi & ~atomicOr(a.chg + w0 + 1, hi));
         a.ctr->update_flag = 1u;
       }
       if (j < rows && MODE == kRowFilter && row_active(j)) {
@@ -255,9 +255,86 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(sweep_args<OffT> a) {
   cp_async_wait<0>();
   n_act = __reduce_add_sync(kFull, n_act);
   n_edges = __reduce_add_sync(kFull, n_edges);
+  n_chg = __reduce_add_sync(kFull, n_chg);
   if (lane == 0) {
     if (n_act) atomicAdd(&a.ctr->active, (unsigned long long)n_act);
     if (n_edges) atomicAdd(&a.ctr->edges, (unsigned long long)n_edges);
+    if (n_chg) atomicAdd(&a.ctr->changed, (unsigned long long)n_chg);
+  }
+}
+
+// Dense activation: the same staged tiles over the activation adjacency
+// (rows = changed candidates, C = targets); every edge of a row whose bit is
+// set in chg ORs its target's bit into wr.  gate: 2 = run only when the
+// activation is dense (see pull_args), 1 = only when sparse, 0 = always.
+template <typename OffT>
+__global__ void __launch_bounds__(kSweepThreads) k_expand_sweep(sweep_args<OffT> a) {
+  if (a.ctr->done) return;
+  if (a.gate == 2 && !changed_dense(a.ctr, a.gate_cur, a.dense_edges)) return;
+  // Here rd = the changed rows, chg = the frontier being written.
+  extern __shared__ __align__(16) unsigned char smem[];
+  const uint32_t rwords = (kTileItems + 8) * sizeof(OffT) / 4;
+  uint32_t *base = reinterpret_cast<uint32_t *>(smem);
+  OffT *Rs[2];
+  uint32_t *Cs[2];
+  for (int b = 0; b < 2; ++b) {
+    uint32_t *p = base + b * (rwords + 2 * kStageWords);
+    Rs[b] = reinterpret_cast<OffT *>(p);
+    Cs[b] = p + rwords;
+  }
+  const uint32_t tid = threadIdx.x, lane = lane_id();
+  uint32_t n_rows = 0, n_edges = 0;
+  const uint64_t stride = gridDim.x;
+  uint64_t t = blockIdx.x;
+  if (t < a.ntiles) stage_tile<OffT, false>(a, tile_of(a, t), Rs[0], Cs[0], nullptr);
+  cp_async_commit();
+  int buf = 0;
+  for (; t < a.ntiles; t += stride, buf ^= 1) {
+    const tile_geom<OffT> g = tile_of(a, t);
+    const uint64_t tn = t + stride;
+    if (tn < a.ntiles) stage_tile<OffT, false>(a, tile_of(a, tn), Rs[buf ^ 1], Cs[buf ^ 1], nullptr);
+    cp_async_commit();
+    cp_async_wait<1>();
+    __syncthreads();
+    const uint32_t rows = (uint32_t)(g.v1 - g.v0 + 1);
+    const OffT *R_t = Rs[buf] + (g.v0 - g.r_al);
+    const uint32_t *C_t = Cs[buf] + (g.e_lo - g.e_al);
+    const uint64_t x0 = g.item_lo + (uint64_t)tid * kItemsPerThread;
+    const uint64_t x1 = min(x0 + (uint64_t)kItemsPerThread, g.item_hi);
+    if (x0 < x1) {
+      uint32_t lo = 0, hi = rows;
+      while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (g.v0 + mid + (uint64_t)R_t[mid] <= x0) lo = mid; else hi = mid;
+      }
+      uint32_t r = lo;
+      bool on = (a.rd[(g.v0 + r) >> 5] >> ((g.v0 + r) & 31u)) & 1u;
+#pragma unroll
+      for (int k = 0; k < kItemsPerThread; ++k) {
+        const uint64_t x = x0 + k;
+        if (x >= x1) break;
+        if (r + 1 <= rows && g.v0 + r + 1 + (uint64_t)R_t[r + 1] == x) {
+          ++r;
+          const uint64_t v = g.v0 + r;
+          on = (a.rd[v >> 5] >> (v & 31u)) & 1u;
+          n_rows += on ? 1u : 0u;
+          continue;
+        }
+        if (!on) continue;
+        const uint64_t e = x - (g.v0 + r) - 1;
+        const uint32_t tgt = C_t[e - g.e_lo];
+        atomicOr(a.chg + (tgt >> 5), 1u << (tgt & 31u));
+        ++n_edges;
+      }
+    }
+    __syncthreads();
+  }
+  cp_async_wait<0>();
+  n_rows = __reduce_add_sync(kFull, n_rows);
+  n_edges = __reduce_add_sync(kFull, n_edges);
+  if (lane == 0) {
+    if (n_rows) atomicAdd(&a.ctr->updated, (unsigned long long)n_rows);
+    if (n_edges) atomicAdd(&a.ctr->out_edges, (unsigned long long)n_edges);
   }
 }
 

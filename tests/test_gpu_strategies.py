@@ -119,6 +119,55 @@ def test_selector_record_train_and_run(engine, uploaded):
     engine.selector_load(forced_selector(0))
 
 
+def test_autotune_keeps_results(engine):
+    n = 1 << 15
+    s, d, w = capi.gen_rmat(15, 16 << 15, seed=41)
+    R, C, E = capi.csc_from_edges(n, s, d, w)
+    g = capi.Graph(engine, R, C, E)
+    srcs = np.array([1, 2, 3, 4], np.uint32)
+    r = g.autotune(srcs, batch=16)
+    assert r.batch_chunk_items in (128, 256, 512, 1024, 2048)
+    assert r.tpv_strategy in (capi.STRATEGY_TPV1, capi.STRATEGY_TPV4, capi.STRATEGY_TPV8,
+                              capi.STRATEGY_TPV32)
+    assert r.trials > 10 and r.plain_ms > 0 and r.batch_ms > 0
+    for strategy in (capi.STRATEGY_PLAIN, capi.STRATEGY_AUTO):
+        dist, _ = g.sssp(9, opts=capi.default_opts(strategy=strategy))
+        V0 = np.full(n, INF, np.uint32)
+        V0[9] = 0
+        want, _ = O.sanity_check(R, C, E, V0, op=O.OP_SSSP_SAT)
+        np.testing.assert_array_equal(dist, want)
+    bd, _ = g.sssp_batch(np.arange(16, dtype=np.uint32) * 7)
+    for j in (0, 5):
+        V0 = np.full(n, INF, np.uint32)
+        V0[j * 7] = 0
+        want, _ = O.sanity_check(R, C, E, V0, op=O.OP_SSSP_SAT)
+        np.testing.assert_array_equal(bd[:, j], want)
+
+
+@pytest.mark.parametrize("dense", [0, 1])
+def test_plain_sweep_gate_both_paths(engine, dense):
+    """Force the plain loop's pull and activation onto the staged sweeps
+    (dense) or the chunked kernels (sparse) for every iteration."""
+    n = 1 << 14
+    s, d, w = capi.gen_rmat(14, 16 << 14, seed=43)
+    R, C, E = capi.csc_from_edges(n, s, d, w)
+    g = capi.Graph(engine, R, C, E)
+    tune = capi.load().kites_graph_set_density
+    capi._check(tune(g._h, 0 if dense else 1 << 62, 0 if dense else 1 << 62))
+    for strategy in (capi.STRATEGY_PLAIN, capi.STRATEGY_AUTO):
+        for dl in (0, 1):
+            dist, _ = g.sssp(5, opts=capi.default_opts(strategy=strategy, device_loop=dl))
+            V0 = np.full(n, INF, np.uint32)
+            V0[5] = 0
+            want, _ = O.sanity_check(R, C, E, V0, op=O.OP_SSSP_SAT)
+            np.testing.assert_array_equal(dist, want)
+    bd, _ = g.sssp_batch(np.arange(16, dtype=np.uint32) + 3)
+    V0 = np.full(n, INF, np.uint32)
+    V0[3] = 0
+    want, _ = O.sanity_check(R, C, E, V0, op=O.OP_SSSP_SAT)
+    np.testing.assert_array_equal(bd[:, 0], want)
+
+
 def test_selector_rejects_bad_sizes(engine):
     with pytest.raises(capi.KitesError):
         engine.selector_load(np.zeros(10, np.float32))
