@@ -59,7 +59,7 @@ struct run_counters {
   unsigned long long changed;         // rows marked changed by the pull/push kernels
   unsigned long long last_changed;
   uint32_t sel;                       // strategy class picked for the next iteration
-  uint32_t pad1;
+  uint32_t error;                     // a kernel's self-check failed (bad staged index)
 };
 
 // ---- warp primitives ---------------------------------------------------

@@ -593,6 +593,7 @@ int run_plain(kites_graph *g, const kites_run_opts &o, kites_run_stats *st) {
     st->kernel_launches += launches;
     if (o.record_iterations) KITES_TRY(record_iterations(g, c, KITES_STRATEGY_PLAIN, st));
   }
+  if (c.error) return fail(KITES_ERR_CUDA, "a kernel self-check failed (staged index)");
   if (c.timed_out)
     return fail(KITES_ERR_TIMEOUT, "no fixed point after %llu iterations",
                 (unsigned long long)c.iterations);
@@ -797,6 +798,7 @@ int run_flex(kites_graph *g, const kites_run_opts &o, kites_run_stats *st) {
     if (o.record_iterations) KITES_TRY(record_iterations(g, c, strategy, st));
     st->host_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   }
+  if (c.error) return fail(KITES_ERR_CUDA, "a kernel self-check failed (staged index)");
   if (c.timed_out)
     return fail(KITES_ERR_TIMEOUT, "no fixed point after %llu iterations",
                 (unsigned long long)c.iterations);
@@ -1013,6 +1015,7 @@ int run_auto(kites_graph *g, const kites_run_opts &o, kites_run_stats *st) {
     }
     st->host_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   }
+  if (c.error) return fail(KITES_ERR_CUDA, "a kernel self-check failed (staged index)");
   if (c.timed_out)
     return fail(KITES_ERR_TIMEOUT, "no fixed point after %llu iterations",
                 (unsigned long long)c.iterations);
@@ -1252,6 +1255,7 @@ int run_batch(kites_graph *g, const uint32_t *sources, uint32_t *dist_out,
     if (o.record_iterations) KITES_TRY(record_iterations(g, c, KITES_STRATEGY_PLAIN, st));
     st->host_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   }
+  if (c.error) return fail(KITES_ERR_CUDA, "a kernel self-check failed (staged index)");
   if (c.timed_out)
     return fail(KITES_ERR_TIMEOUT, "no fixed point after %llu iterations",
                 (unsigned long long)c.iterations);

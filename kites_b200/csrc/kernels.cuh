@@ -390,7 +390,7 @@ __global__ void k_loop_check(run_counters *c, iter_record rec,
   c->total_out_edges += c->out_edges;
   c->active = c->edges = c->updated = c->out_edges = 0;
   bool stop = false;
-  if (c->update_flag == 0) {
+  if (c->update_flag == 0 || c->error) {
     stop = true;
   } else {
     c->update_flag = 0;

@@ -69,10 +69,15 @@ __device__ __forceinline__ tile_geom<OffT> tile_of(const sweep_args<OffT> &a, ui
   g.v0 = a.tile_v0[t];
   g.v1 = a.tile_v0[t + 1];
   if (g.v1 >= a.n_rows) g.v1 = a.n_rows - 1;
+  // First edge item at or after item_lo: item_lo itself is in row v0's
+  // span.  Edge items before item_hi: item_hi minus the vertex items before
+  // it, i.e. rows v0 .. v1 when row v1's vertex item lies inside the tile,
+  // else rows v0 .. v1-1 (then the tile ends exactly at R[v1]).
   const int64_t r0 = (int64_t)a.R[g.v0];
-  const int64_t r1 = (int64_t)a.R[g.v1 + 1];
+  const int64_t rv1 = (int64_t)a.R[g.v1];
   g.e_lo = (uint64_t)max(r0, (int64_t)g.item_lo - (int64_t)g.v0 - 1);
-  g.e_hi = (uint64_t)min(r1, (int64_t)g.item_hi - (int64_t)g.v1 - 1);
+  const bool v1_inside = (uint64_t)((int64_t)g.v1 + rv1) < g.item_hi;
+  g.e_hi = v1_inside ? g.item_hi - g.v1 - 1 : (uint64_t)rv1;
   if (g.e_hi < g.e_lo) g.e_hi = g.e_lo;
   const uint64_t per16 = 16 / sizeof(uint32_t);
   g.e_al = g.e_lo & ~(per16 - 1);
@@ -175,10 +180,15 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(sweep_args<OffT> a) {
           row_on = row_active(r);
           continue;
         }
+        if (x == g.v0 + r + (uint64_t)R_t[r]) continue;  // the start row's own vertex item
         const uint64_t e = x - (g.v0 + r) - 1;  // global edge index
         crow[k] = r;
         if (!row_on) continue;
         const uint32_t u = C_t[e - g.e_lo];
+        if (u >= a.n_rows || e >= g.e_hi) {  // staged slice out of step: never gather
+          a.ctr->error = 1u;
+          continue;
+        }
         if (MODE == kEdgeFilter && !((a.U[u >> 5] >> (u & 31u)) & 1u)) continue;
         const uint32_t w = kW ? E_t[e - g.e_lo] : 0u;
         cand[k] = nbr_comp<OP>(a.V[u], w);
@@ -320,9 +330,17 @@ __global__ void __launch_bounds__(kSweepThreads) k_expand_sweep(sweep_args<OffT>
           n_rows += on ? 1u : 0u;
           continue;
         }
+        if (x == g.v0 + r + (uint64_t)R_t[r]) {  // the start row's own vertex item
+          n_rows += on ? 1u : 0u;
+          continue;
+        }
         if (!on) continue;
         const uint64_t e = x - (g.v0 + r) - 1;
         const uint32_t tgt = C_t[e - g.e_lo];
+        if (tgt >= a.n_rows || e >= g.e_hi) {  // staged slice out of step
+          a.ctr->error = 1u;
+          continue;
+        }
         atomicOr(a.chg + (tgt >> 5), 1u << (tgt & 31u));
         ++n_edges;
       }
