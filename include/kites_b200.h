@@ -218,6 +218,23 @@ int kites_sssp_multi_seed(kites_engine *eng, kites_graph *g, int op, const uint3
                           uint64_t n_seeds, uint32_t *dist_out, const kites_run_opts *opts,
                           kites_run_stats *stats);
 
+/* Single-source saturating SSSP that allocates no device memory, for callers
+ * that cannot allocate when they need an answer (memory reserved up front
+ * with allocation forbidden on the serving path, or device memory owned by
+ * another runtime's allocator).  No counterpart in the reference.
+ * The caller owns every buffer: the CSC (R: n+1 uint32 offsets, C, E:
+ * n_edges uint32), the out-adjacency (out_R, out_C: destinations of each
+ * source, n_edges entries) and dist (n uint32), all device pointers; stream
+ * may be NULL.  Scratch (two frontier bitmaps, flags) is a fixed 4 MiB + 256 B
+ * array compiled into the library, held by every GPU that loads it until the
+ * process exits; hence n_vertices <= 16,777,216 (larger sizes are rejected).
+ * The first call on a device looks that array's address up and should come
+ * before any stream capture.  Calls share the array: calls that overlap on
+ * the GPU race.  Validates the graph on the device before traversing it. */
+int kites_sssp_noalloc(const uint32_t *R, const uint32_t *C, const uint32_t *E, uint64_t n_edges,
+                       const uint32_t *out_R, const uint32_t *out_C, uint32_t n_vertices,
+                       uint32_t source, uint32_t *dist, void *stream, uint32_t *iterations);
+
 /* Min-label connected components: V[v] = v, every vertex active. */
 int kites_cc(kites_engine *eng, kites_graph *g, uint32_t *labels_out,
              const kites_run_opts *opts, kites_run_stats *stats);

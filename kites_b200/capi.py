@@ -37,7 +37,7 @@ EXPORTED = [
     "kites_csc_from_edges", "kites_selector_record", "kites_selector_train",
     "kites_selector_load", "kites_selector_save", "kites_graph_set_tpv",
     "kites_sssp_multi_seed", "kites_gen_rmat_union", "kites_autotune",
-    "kites_graph_set_density",
+    "kites_graph_set_density", "kites_sssp_noalloc",
 ]
 SELECTOR_FEATURES, SELECTOR_CLASSES, SELECTOR_PARAMS = 12, 4, 1628
 # Parameter layout of the selector MLP (offsets into the 1628 floats).
@@ -161,6 +161,8 @@ def load(path: str = LIB_PATH):
                                          vp, vp]),
         "kites_autotune": (c_int, [vp, vp, c_int, vp, u32, u32, POINTER(TuneResult)]),
         "kites_graph_set_density": (c_int, [vp, u64, u64]),
+        "kites_sssp_noalloc": (c_int, [vp, vp, vp, u64, vp, vp, u32, u32, vp, vp,
+                                       POINTER(c_uint32)]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)

@@ -23,6 +23,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
 #include <mutex>
 
 #include "common.cuh"
@@ -145,6 +146,21 @@ __global__ void __launch_bounds__(kNaWarps * 32)
   }
 }
 
+// Caller graph check before any traversal: offsets start at 0, never
+// decrease and end at the edge count; every id is below n.  Sets bits of
+// *err instead of letting a bad index reach a gather or a bitmap write.
+__global__ void k_na_validate(const uint32_t *__restrict__ R, const uint32_t *__restrict__ C,
+                              uint64_t n, uint64_t m, uint32_t *err) {
+  const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = tid; i < n; i += stride) {
+    const uint32_t a = R[i], b = R[i + 1];
+    if (a > b || (i == 0 && a != 0) || (i + 1 == n && (uint64_t)b != m)) atomicOr(err, 1u);
+  }
+  for (uint64_t i = tid; i < m; i += stride)
+    if (C[i] >= n) atomicOr(err, 2u);
+}
+
 __global__ void k_na_clear(uint32_t *p, uint64_t words) {
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < words;
        i += (uint64_t)gridDim.x * blockDim.x)
@@ -175,12 +191,13 @@ int noalloc_scratch(unsigned char **out) {
 using namespace kites_internal;
 
 extern "C" int kites_sssp_noalloc(const uint32_t *R, const uint32_t *C, const uint32_t *E,
-                                  const uint32_t *out_R, const uint32_t *out_C,
-                                  uint32_t n_vertices, uint32_t source, uint32_t *dist,
-                                  void *stream, uint32_t *iterations) {
+                                  uint64_t n_edges, const uint32_t *out_R,
+                                  const uint32_t *out_C, uint32_t n_vertices, uint32_t source,
+                                  uint32_t *dist, void *stream, uint32_t *iterations) {
   clear_error();
   if (!R || !C || !E || !out_R || !out_C || !dist)
     return fail(KITES_ERR_INVALID, "null graph or output pointer");
+  if (n_edges > 0xFFFFFFFFull) return fail(KITES_ERR_INVALID, "32-bit offsets: < 2^32 edges");
   if (n_vertices == 0 || (uint64_t)n_vertices > kNoAllocMaxVertices)
     return fail(KITES_ERR_INVALID,
                 "kites_sssp_noalloc takes 1 .. %llu vertices (its fixed scratch holds two "
@@ -193,8 +210,18 @@ extern "C" int kites_sssp_noalloc(const uint32_t *R, const uint32_t *C, const ui
   const uint64_t n = n_vertices;
   const uint64_t words = (n + 31) / 32;
   uint32_t *flag = reinterpret_cast<uint32_t *>(scratch);
+  uint32_t *err = flag + 1;
   uint32_t *bits = reinterpret_cast<uint32_t *>(scratch + kNoAllocHeader);
   uint32_t *frontier[2] = {bits, bits + words};
+  KITES_CUDA_TRY(cudaMemsetAsync(err, 0, sizeof(uint32_t), s));
+  k_na_validate<<<1184, 256, 0, s>>>(R, C, n, n_edges, err);
+  k_na_validate<<<1184, 256, 0, s>>>(out_R, out_C, n, n_edges, err);
+  uint32_t host_err = 0;
+  KITES_CUDA_TRY(cudaMemcpyAsync(&host_err, err, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  KITES_CUDA_TRY(cudaStreamSynchronize(s));
+  if (host_err & 1u)
+    return fail(KITES_ERR_INVALID, "offsets are not 0 .. n_edges and non-decreasing");
+  if (host_err & 2u) return fail(KITES_ERR_INVALID, "a vertex id is >= n_vertices");
   k_na_init<<<592, 256, 0, s>>>(dist, n, bits, words, flag);
   k_na_seed<<<32, 256, 0, s>>>(dist, source, out_R, out_C, frontier[0]);
   KITES_CUDA_TRY(cudaGetLastError());
