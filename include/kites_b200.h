@@ -178,6 +178,17 @@ int kites_engine_stream(kites_engine *eng, void **stream_out);
  * B200 layout (edge-balanced chunk table, weighted out-CSR). */
 int kites_graph_upload(kites_engine *eng, const kites_csc_view *view,
                        kites_graph **out);
+/* Builds the CSC of an edge list on the device and uploads it, like
+ * kites_graph_upload of the CSC that graph_raw::construct_me
+ * (kites/graph/graph_raw.h:57-190) sorts on the host: rows keyed by
+ * destination, each row's sources ascending, parallel edges kept in input
+ * order.  src, dst, weights (NULL: unweighted): n_edges uint32 each, host or
+ * device memory; n_edges < 2^31.  directed = 0 expects both directions of
+ * every undirected edge in the list; vpg 1, vertex values 4 bytes, no
+ * initial values or frontier (set them with kites_graph_set_*). */
+int kites_graph_from_edges(kites_engine *eng, uint64_t n_vertices, uint64_t n_edges,
+                           const uint32_t *src, const uint32_t *dst, const uint32_t *weights,
+                           int directed, kites_graph **out);
 int kites_graph_destroy(kites_graph *g);
 int kites_graph_device_view(kites_graph *g, kites_device_view *out);
 /* Copy vertex values in or out (host or device pointer, cudaMemcpyDefault),

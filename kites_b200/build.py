@@ -30,6 +30,7 @@ CXX_FLAGS = ["-O3", "-std=c++17", "-fPIC", "-fopenmp", "-I", INCLUDE, "-I", CSRC
 
 def _deps(src: str) -> list[str]:
     hdrs = glob.glob(os.path.join(CSRC, "*.h")) + glob.glob(os.path.join(CSRC, "*.cuh"))
+    hdrs += glob.glob(os.path.join(CSRC, "*.inc"))
     hdrs += glob.glob(os.path.join(INCLUDE, "*.h"))
     return [src] + hdrs
 

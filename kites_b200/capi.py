@@ -37,7 +37,7 @@ EXPORTED = [
     "kites_csc_from_edges", "kites_selector_record", "kites_selector_train",
     "kites_selector_load", "kites_selector_save", "kites_graph_set_tpv",
     "kites_sssp_multi_seed", "kites_gen_rmat_union", "kites_autotune",
-    "kites_graph_set_density", "kites_sssp_noalloc",
+    "kites_graph_set_density", "kites_sssp_noalloc", "kites_graph_from_edges",
 ]
 SELECTOR_FEATURES, SELECTOR_CLASSES, SELECTOR_PARAMS = 12, 4, 1628
 # Parameter layout of the selector MLP (offsets into the 1628 floats).
@@ -163,6 +163,7 @@ def load(path: str = LIB_PATH):
         "kites_graph_set_density": (c_int, [vp, u64, u64]),
         "kites_sssp_noalloc": (c_int, [vp, vp, vp, u64, vp, vp, u32, u32, vp, vp,
                                        POINTER(c_uint32)]),
+        "kites_graph_from_edges": (c_int, [vp, u64, u64, vp, vp, vp, c_int, vp]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)
@@ -321,6 +322,30 @@ class Graph:
         self.n_edges = int(v.n_edges)
         dv = self.device_view()
         self.n_padded = int(dv.n_vertices)
+
+    @classmethod
+    def from_edges(cls, engine: Engine, n_vertices, src, dst, w=None, directed=True):
+        """CSC built on the device from an edge list (kites_graph_from_edges);
+        src/dst/w are numpy arrays or device pointers with n_edges given by
+        len(src)."""
+        self = cls.__new__(cls)
+        self.engine = engine
+        if hasattr(src, "ctypes"):
+            src = np.ascontiguousarray(src, dtype=np.uint32)
+            dst = np.ascontiguousarray(dst, dtype=np.uint32)
+            if w is not None:
+                w = np.ascontiguousarray(w, dtype=np.uint32)
+        m = len(src)
+        self._keep = None
+        self._h = c_void_p()
+        _check(load().kites_graph_from_edges(engine._h, int(n_vertices), m, _p(src), _p(dst),
+                                             _p(w), 1 if directed else 0,
+                                             ctypes.byref(self._h)))
+        engine._graphs.add(self)
+        self.n_vertices = int(n_vertices)
+        self.n_edges = m
+        self.n_padded = int(self.device_view().n_vertices)
+        return self
 
     def close(self):
         if self._h:

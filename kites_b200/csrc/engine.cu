@@ -30,6 +30,18 @@ char *error_buffer() {
 
 namespace {
 
+// Default selector weights: written by `python -m kites_b200.train_selector
+// --inc`, trained on generated graphs; without the file a fresh engine has
+// neutral weights (always PLAIN).
+#if __has_include("selector_default.inc")
+#define KITES_HAVE_DEFAULT_SELECTOR 1
+static const float kDefaultSelector[] = {
+#include "selector_default.inc"
+};
+static_assert(sizeof(kDefaultSelector) == kParams * sizeof(float),
+              "selector_default.inc must hold the 1628 selector parameters");
+#endif
+
 int dev_alloc(kites_engine *eng, void **p, size_t bytes) {
   *p = nullptr;
   // At least 16 bytes of slack past the end: the staged sweep copies whole
@@ -1373,7 +1385,16 @@ extern "C" int kites_engine_create(int device, kites_engine **out) {
       st = fail(KITES_ERR_OOM, "selector allocation failed: %s", cudaGetErrorString(ce));
       break;
     }
+#ifdef KITES_HAVE_DEFAULT_SELECTOR
+    ce = cudaMemcpyAsync(eng->sel_params, kDefaultSelector, sizeof(kDefaultSelector),
+                         cudaMemcpyHostToDevice, eng->stream);
+    if (ce != cudaSuccess) {
+      st = fail(KITES_ERR_CUDA, "selector init failed: %s", cudaGetErrorString(ce));
+      break;
+    }
+#else
     k_mlp_neutral<<<1, 256, 0, eng->stream>>>(eng->sel_params);
+#endif
     if ((ce = cudaStreamSynchronize(eng->stream)) != cudaSuccess) {
       st = fail(KITES_ERR_CUDA, "selector init failed: %s", cudaGetErrorString(ce));
       break;
@@ -1523,6 +1544,142 @@ extern "C" int kites_graph_upload(kites_engine *eng, const kites_csc_view *v,
   }
   *out = g;
   return KITES_OK;
+}
+
+// ---- device-side ingestion (edge list -> CSC) -----------------------------
+
+// keys[i] = dst << 32 | src; any endpoint >= n sets *bad.
+__global__ void k_edge_keys(const uint32_t *__restrict__ src, const uint32_t *__restrict__ dst,
+                            uint64_t m, uint64_t n, uint64_t *__restrict__ keys, uint32_t *bad) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t s = src[i], d = dst[i];
+    if (s >= n || d >= n) atomicOr(bad, 1u);
+    keys[i] = (uint64_t)d << 32 | s;
+  }
+}
+
+// R[d] = first sorted edge whose destination is >= d (binary search), for
+// d in [0, n]; C[i] = source of sorted edge i.
+__global__ void k_rows_of_keys(const uint64_t *__restrict__ keys, uint64_t m, uint64_t n,
+                               uint64_t *__restrict__ R, uint32_t *__restrict__ C) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t d = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; d <= n; d += stride) {
+    uint64_t lo = 0, hi = m;  // first index with key >> 32 >= d
+    while (lo < hi) {
+      const uint64_t mid = (lo + hi) >> 1;
+      if ((keys[mid] >> 32) < d) lo = mid + 1; else hi = mid;
+    }
+    R[d] = lo;
+  }
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += stride)
+    C[i] = (uint32_t)keys[i];
+}
+
+// Builds the CSC of an edge list on the device -- rows keyed by
+// destination, each row's sources ascending, parallel edges kept in input
+// order (a stable radix sort of dst << 32 | src) -- and uploads it as
+// kites_graph_upload does.  The edge arrays may be host or device memory.
+extern "C" int kites_graph_from_edges(kites_engine *eng, uint64_t n_vertices, uint64_t n_edges,
+                                      const uint32_t *src, const uint32_t *dst,
+                                      const uint32_t *weights, int directed,
+                                      kites_graph **out) {
+  clear_error();
+  if (!eng || !out) return fail(KITES_ERR_INVALID, "null argument");
+  *out = nullptr;
+  if (n_vertices == 0 || n_vertices >= 0xFFFFFF00ull)
+    return fail(KITES_ERR_INVALID, "n_vertices must be in 1 .. 2^32 - 256");
+  if (n_edges && (!src || !dst)) return fail(KITES_ERR_INVALID, "null edge arrays");
+  if (n_edges > 0x7FFFFFFFull)
+    return fail(KITES_ERR_UNSUPPORTED, "device ingestion takes < 2^31 edges");
+  KITES_TRY(set_device(eng));
+  cudaStream_t s = eng->stream;
+  const uint64_t m = n_edges, n = n_vertices;
+  void *p = nullptr;
+  uint64_t *keys[2] = {nullptr, nullptr}, *R = nullptr;
+  uint32_t *ends[2] = {nullptr, nullptr}, *w[2] = {nullptr, nullptr}, *C = nullptr, *bad = nullptr;
+  void *temp = nullptr;
+  std::vector<void *> tmp;
+  auto alloc = [&](void **q, size_t bytes) {
+    int st = dev_alloc(eng, q, bytes);
+    if (st == KITES_OK) tmp.push_back(*q);
+    return st;
+  };
+  int st = KITES_OK;
+  do {
+    const size_t mm = (size_t)std::max<uint64_t>(m, 1);
+    if ((st = alloc(&p, mm * 8)) != KITES_OK) break;
+    keys[0] = (uint64_t *)p;
+    if ((st = alloc(&p, mm * 8)) != KITES_OK) break;
+    keys[1] = (uint64_t *)p;
+    if ((st = alloc(&p, (n + 1) * 8)) != KITES_OK) break;
+    R = (uint64_t *)p;
+    if ((st = alloc(&p, mm * 4)) != KITES_OK) break;
+    C = (uint32_t *)p;
+    if ((st = alloc(&p, 4)) != KITES_OK) break;
+    bad = (uint32_t *)p;
+    if (weights) {
+      if ((st = alloc(&p, mm * 4)) != KITES_OK) break;
+      w[0] = (uint32_t *)p;
+      if ((st = alloc(&p, mm * 4)) != KITES_OK) break;
+      w[1] = (uint32_t *)p;
+    }
+    cudaError_t e = cudaMemsetAsync(bad, 0, 4, s);
+    if (m) {
+      // The endpoints pass through the second key buffer (2 x 4 bytes an edge).
+      ends[0] = (uint32_t *)keys[1];
+      ends[1] = ends[0] + m;
+      if (e == cudaSuccess) e = cudaMemcpyAsync(ends[0], src, m * 4, cudaMemcpyDefault, s);
+      if (e == cudaSuccess) e = cudaMemcpyAsync(ends[1], dst, m * 4, cudaMemcpyDefault, s);
+      if (e == cudaSuccess && weights)
+        e = cudaMemcpyAsync(w[0], weights, m * 4, cudaMemcpyDefault, s);
+      if (e != cudaSuccess) { st = fail(KITES_ERR_CUDA, "edge copy: %s", cudaGetErrorString(e)); break; }
+      k_edge_keys<<<grid_for(m), 256, 0, s>>>(ends[0], ends[1], m, n, keys[0], bad);
+      uint32_t hbad = 0;
+      e = cudaMemcpyAsync(&hbad, bad, 4, cudaMemcpyDeviceToHost, s);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+      if (e != cudaSuccess) { st = fail(KITES_ERR_CUDA, "edge keys: %s", cudaGetErrorString(e)); break; }
+      if (hbad) { st = fail(KITES_ERR_INVALID, "edge endpoint >= n_vertices"); break; }
+      int end_bit = 33;
+      while (end_bit < 64 && (1ull << (end_bit - 32)) < n) ++end_bit;
+      size_t temp_bytes = 0;
+      if (weights)
+        e = cub::DeviceRadixSort::SortPairs(nullptr, temp_bytes, keys[0], keys[1], w[0], w[1],
+                                            (int)m, 0, end_bit, s);
+      else
+        e = cub::DeviceRadixSort::SortKeys(nullptr, temp_bytes, keys[0], keys[1], (int)m, 0,
+                                           end_bit, s);
+      if (e != cudaSuccess) { st = fail(KITES_ERR_CUDA, "sort: %s", cudaGetErrorString(e)); break; }
+      if ((st = alloc(&temp, temp_bytes)) != KITES_OK) break;
+      if (weights)
+        e = cub::DeviceRadixSort::SortPairs(temp, temp_bytes, keys[0], keys[1], w[0], w[1],
+                                            (int)m, 0, end_bit, s);
+      else
+        e = cub::DeviceRadixSort::SortKeys(temp, temp_bytes, keys[0], keys[1], (int)m, 0,
+                                           end_bit, s);
+      if (e != cudaSuccess) { st = fail(KITES_ERR_CUDA, "sort: %s", cudaGetErrorString(e)); break; }
+    }
+    k_rows_of_keys<<<grid_for(n + 1), 256, 0, s>>>(keys[1], m, n, R, C);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) { st = fail(KITES_ERR_CUDA, "rows: %s", cudaGetErrorString(e)); break; }
+    kites_csc_view v = {};
+    v.n_vertices = n;
+    v.n_edges = m;
+    v.row_offsets = R;
+    v.col_indices = C;
+    v.edge_values = weights ? w[1] : nullptr;
+    v.edge_value_size = weights ? 4 : 0;
+    v.vertex_value_size = 4;
+    v.vertex_per_group = 1;
+    v.directed = directed ? 1 : 0;
+    v.on_device = 1;
+    st = kites_graph_upload(eng, &v, out);
+  } while (0);
+  for (void *q : tmp) cudaFreeAsync(q, s);
+  cudaError_t e = cudaStreamSynchronize(s);
+  if (st == KITES_OK && e != cudaSuccess)
+    st = fail(KITES_ERR_CUDA, "ingestion: %s", cudaGetErrorString(e));
+  return st;
 }
 
 extern "C" int kites_graph_device_view(kites_graph *g, kites_device_view *o) {

@@ -1,40 +1,37 @@
-// kernels_sweep.cuh -- shared-memory-staged dense sweep over the CSC.
+// kernels_sweep.cuh -- the tiled dense sweep over the CSC.
 //
-// For iterations where most rows (or most sources) are live, walking the CSC
-// tile by tile beats per-row discovery: a CTA stages a tile of the merged
-// "row, then its in-edges" sequence -- the tile's row offsets and the
-// contiguous slice of C and E -- into shared memory with 16-byte cp.async
-// copies, double-buffered so the next tile streams in while this one is
-// reduced.  Each thread then owns kItemsPerThread consecutive items
-// (merge-path split, found by a binary search over the staged offsets) and
-// issues all of its V[u] gathers back to back.  Row partials meet in a
-// shared-memory accumulator: rows interior to a thread store directly,
-// rows at thread boundaries are pre-reduced over the warp (runs of equal
-// row) and merged with shared atomicMin; rows split across tiles merge
+// For iterations where most rows (or most sources) are live, walking the
+// CSC tile by tile beats per-row discovery.  A tile is kTileItems
+// consecutive items of the merged "row, then its in-edges" sequence (row v
+// at item v + R[v], its edge e at v + 1 + e).  A CTA first marks the tile's
+// vertex items in a shared bitmap (one bit per item) and records each row's
+// local position; then every warp walks 8 windows of 32 consecutive items,
+// one item per lane.  A lane's row is the number of vertex items up to it
+// (prefix popcounts of the bitmap), its edge index follows from the row, so
+// the loads of C and E are coalesced and every lane has all of its gathers
+// in flight together.  Row minima meet in a shared accumulator through the
+// warp-segmented min (runs of equal row) and shared atomicMin; rows that
+// lie wholly in the tile store their value, rows split across tiles merge
 // into V with global atomicMin.
 //
 // Modes: kRowFilter -- rows whose frontier bit is set (PLAIN on a dense
 // frontier); kEdgeFilter -- every row, only in-edges whose source changed
-// last iteration (PULL_ALL).
+// last iteration (PULL_ALL).  k_expand_sweep is the same walk over the
+// activation adjacency.
 #pragma once
 #include "kernels.cuh"
 
 namespace kites_internal {
 
 constexpr int kSweepThreads = 256;
-constexpr int kItemsPerThread = 8;
-constexpr int kTileItems = kSweepThreads * kItemsPerThread;  // 2048
-constexpr int kStageWords = kTileItems + 8;                  // + 16-byte alignment slack
+constexpr int kSweepWarps = kSweepThreads / 32;
+constexpr int kWindows = 8;                                   // windows of 32 items per warp
+constexpr int kTileItems = kSweepWarps * kWindows * 32;       // 2048
+constexpr int kTileWords = kTileItems / 32;                   // vertex-item bitmap words
+constexpr int kRowSlots = kTileItems + 4;                     // rows + 1 <= 2050
+constexpr int kFrontierWords = 72;                            // bitmap words of <= 2049 rows
 
 enum { kRowFilter = 0, kEdgeFilter = 1 };
-
-__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
-  const uint32_t s = (uint32_t)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
 
 template <typename OffT>
 struct sweep_args {
@@ -44,225 +41,205 @@ struct sweep_args {
   uint32_t *V;
   const uint32_t *tile_v0;   // chunk table with kTileItems items per chunk
   uint64_t ntiles, n_rows, n_items;
-  const uint32_t *rd;        // kRowFilter: frontier bits
+  const uint32_t *rd;        // kRowFilter: frontier bits (expand: the changed rows)
   const uint32_t *U;         // kEdgeFilter: changed bits of the previous iteration
-  uint32_t *chg;             // next changed bits (vertex level)
+  uint32_t *chg;             // next changed bits (expand: the frontier written)
   run_counters *ctr;
-  uint64_t m;                // edges (bounds of the staged slices)
-  // kRowFilter density gate (see pull_args): 2 = run only on dense frontiers.
+  uint64_t m;                // edges
+  // Density gate (see pull_args / expand_args): 2 = run only when dense.
   uint32_t gate, gate_cur;
   unsigned long long dense_edges;
 };
 
-template <typename OffT>
+// Shared memory of a sweep CTA (static, < 17 KB).
+struct sweep_smem {
+  int32_t pos[kRowSlots];       // local position of row j's vertex item
+  uint32_t acc[kRowSlots];      // row minima
+  uint32_t isv[kTileWords];     // bit i: item i is a vertex item
+  uint32_t fw[kFrontierWords];  // frontier / changed words of the rows
+};
+
 struct tile_geom {
-  uint64_t item_lo, item_hi, v0, v1;  // rows v0..v1 (inclusive)
-  uint64_t e_lo, e_hi;                // edges of the tile [e_lo, e_hi)
-  uint64_t e_al, r_al;                // 16-byte aligned starts of the staged slices
+  uint64_t item_lo, v0;
+  uint32_t rows, nloc;          // rows v0 .. v0 + rows - 1; items [item_lo, item_lo + nloc)
 };
 
 template <typename OffT>
-__device__ __forceinline__ tile_geom<OffT> tile_of(const sweep_args<OffT> &a, uint64_t t) {
-  tile_geom<OffT> g;
+__device__ __forceinline__ tile_geom tile_of(const sweep_args<OffT> &a, uint64_t t) {
+  tile_geom g;
   g.item_lo = t * (uint64_t)kTileItems;
-  g.item_hi = min(g.item_lo + (uint64_t)kTileItems, a.n_items);
+  g.nloc = (uint32_t)(min(g.item_lo + (uint64_t)kTileItems, a.n_items) - g.item_lo);
   g.v0 = a.tile_v0[t];
-  g.v1 = a.tile_v0[t + 1];
-  if (g.v1 >= a.n_rows) g.v1 = a.n_rows - 1;
-  // First edge item at or after item_lo: item_lo itself is in row v0's
-  // span.  Edge items before item_hi: item_hi minus the vertex items before
-  // it, i.e. rows v0 .. v1 when row v1's vertex item lies inside the tile,
-  // else rows v0 .. v1-1 (then the tile ends exactly at R[v1]).
-  const int64_t r0 = (int64_t)a.R[g.v0];
-  const int64_t rv1 = (int64_t)a.R[g.v1];
-  g.e_lo = (uint64_t)max(r0, (int64_t)g.item_lo - (int64_t)g.v0 - 1);
-  const bool v1_inside = (uint64_t)((int64_t)g.v1 + rv1) < g.item_hi;
-  g.e_hi = v1_inside ? g.item_hi - g.v1 - 1 : (uint64_t)rv1;
-  if (g.e_hi < g.e_lo) g.e_hi = g.e_lo;
-  const uint64_t per16 = 16 / sizeof(uint32_t);
-  g.e_al = g.e_lo & ~(per16 - 1);
-  g.r_al = g.v0 & ~(uint64_t)(16 / sizeof(OffT) - 1);
+  uint64_t v1 = a.tile_v0[t + 1];
+  if (v1 >= a.n_rows) v1 = a.n_rows - 1;
+  g.rows = (uint32_t)(v1 - g.v0 + 1);
   return g;
 }
 
-// Stage R[r_al .. v1+1], C/E[e_al .. e_hi) (rounded up to 16 bytes; the
-// pool rounds every allocation to 256 bytes, so the tail stays inside it).
-template <typename OffT, bool kWeights>
-__device__ __forceinline__ void stage_tile(const sweep_args<OffT> &a, const tile_geom<OffT> &g,
-                                           OffT *Rs, uint32_t *Cs, uint32_t *Es) {
-  const uint32_t tid = threadIdx.x;
-  const uint64_t r_words = (g.v1 + 2 - g.r_al) * sizeof(OffT);        // bytes
-  const uint64_t r_chunks = (r_words + 15) / 16;
-  for (uint64_t i = tid; i < r_chunks; i += kSweepThreads)
-    cp_async16(reinterpret_cast<char *>(Rs) + i * 16,
-               reinterpret_cast<const char *>(a.R + g.r_al) + i * 16);
-  const uint64_t e_chunks = ((g.e_hi - g.e_al) * 4 + 15) / 16;
-  for (uint64_t i = tid; i < e_chunks; i += kSweepThreads) {
-    cp_async16(reinterpret_cast<char *>(Cs) + i * 16,
-               reinterpret_cast<const char *>(a.C + g.e_al) + i * 16);
-    if (kWeights)
-      cp_async16(reinterpret_cast<char *>(Es) + i * 16,
-                 reinterpret_cast<const char *>(a.E + g.e_al) + i * 16);
+// Phase A: pos[j] = v0 + j + R[v0 + j] - item_lo for j in [0, rows], clamped
+// to [-1, kTileItems + 1] (outside the tile only "before" and "after"
+// matter: only row 0 starts before it, only row `rows` after it); the
+// bitmap bit of every vertex item inside the tile; acc = INF; the rows'
+// bitmap words from `bits` (when given).  isv must be zero on entry.
+template <typename OffT>
+__device__ __forceinline__ void tile_setup(const sweep_args<OffT> &a, const tile_geom &g,
+                                           const uint32_t *bits, sweep_smem &sm) {
+  for (uint32_t j = threadIdx.x; j <= g.rows; j += kSweepThreads) {
+    const int64_t p = (int64_t)(g.v0 + j) + (int64_t)a.R[g.v0 + j] - (int64_t)g.item_lo;
+    sm.pos[j] = (int32_t)max((int64_t)-1, min(p, (int64_t)kTileItems + 1));
+    if (p >= 0 && p < (int64_t)g.nloc) atomicOr(&sm.isv[p >> 5], 1u << (p & 31));
+    if (j < g.rows) sm.acc[j] = kInf;
+  }
+  if (bits) {
+    const uint32_t nw = ((uint32_t)(g.v0 & 31u) + g.rows + 31u) >> 5;  // <= 66
+    for (uint32_t i = threadIdx.x; i < nw; i += kSweepThreads) sm.fw[i] = bits[(g.v0 >> 5) + i];
   }
 }
 
+// Per-warp view of the tile: window k of warp w covers items
+// (w * kWindows + k) * 32 + lane.  row(item) = vertex items up to and
+// including it, minus 1 when the tile starts with row v0's vertex item.
+struct window_rows {
+  uint32_t pfx[kWindows];  // vertex items before each window
+  uint32_t adj;
+  __device__ __forceinline__ window_rows(const sweep_smem &sm) {
+    const uint32_t lane = lane_id(), w = threadIdx.x >> 5;
+    const uint32_t c0 = __popc(sm.isv[lane]), c1 = __popc(sm.isv[lane + 32]);
+    const uint32_t s0 = warp_inclusive_scan(c0), s1 = warp_inclusive_scan(c1);
+    const uint32_t t0 = __shfl_sync(kFull, s0, 31);
+    const uint32_t ex0 = s0 - c0, ex1 = t0 + s1 - c1;
+#pragma unroll
+    for (int k = 0; k < kWindows; ++k) {
+      const uint32_t wi = w * kWindows + k;  // warp-uniform
+      pfx[k] = __shfl_sync(kFull, wi < 32 ? ex0 : ex1, wi & 31u);
+    }
+    adj = sm.pos[0] == 0 ? 1u : 0u;
+  }
+};
+
 template <int OP, typename OffT, int MODE>
-__global__ void __launch_bounds__(kSweepThreads) k_sweep(sweep_args<OffT> a) {
+__global__ void __launch_bounds__(kSweepThreads, 4) k_sweep(sweep_args<OffT> a) {
   if (a.ctr->done) return;
   if (a.gate == 2 && !frontier_dense(a.ctr, a.gate_cur, a.dense_edges)) return;
   constexpr bool kW = op_reads_weights<OP>();
-  extern __shared__ __align__(16) unsigned char smem[];
-  // Two stage buffers + the row accumulator.
-  const uint32_t rwords = (kTileItems + 8) * sizeof(OffT) / 4;
-  uint32_t *base = reinterpret_cast<uint32_t *>(smem);
-  OffT *Rs[2];
-  uint32_t *Cs[2], *Es[2];
-  for (int b = 0; b < 2; ++b) {
-    uint32_t *p = base + b * (rwords + 2 * kStageWords);
-    Rs[b] = reinterpret_cast<OffT *>(p);
-    Cs[b] = p + rwords;
-    Es[b] = p + rwords + kStageWords;
-  }
-  uint32_t *acc_s = base + 2 * (rwords + 2 * kStageWords);  // kTileItems + 1 rows
-  const uint32_t tid = threadIdx.x, lane = lane_id();
+  constexpr uint32_t kNone = 0xFFFFFFFFu;
+  __shared__ sweep_smem sm;
+  const uint32_t tid = threadIdx.x, lane = lane_id(), w = tid >> 5;
+  const uint32_t le_mask = kFull >> (31u - lane);  // lanes 0 .. lane
   uint32_t n_act = 0, n_edges = 0, n_chg = 0;
-  const uint64_t stride = gridDim.x;
-  uint64_t t = blockIdx.x;
-  if (t < a.ntiles) stage_tile<OffT, kW>(a, tile_of(a, t), Rs[0], Cs[0], Es[0]);
-  cp_async_commit();
-  int buf = 0;
-  for (; t < a.ntiles; t += stride, buf ^= 1) {
-    const tile_geom<OffT> g = tile_of(a, t);
-    const uint64_t tn = t + stride;
-    if (tn < a.ntiles) stage_tile<OffT, kW>(a, tile_of(a, tn), Rs[buf ^ 1], Cs[buf ^ 1], Es[buf ^ 1]);
-    cp_async_commit();
-    const uint32_t rows = (uint32_t)(g.v1 - g.v0 + 1);
-    for (uint32_t j = tid; j < rows; j += kSweepThreads) acc_s[j] = kInf;
-    cp_async_wait<1>();
+  if (tid < kTileWords) sm.isv[tid] = 0u;
+  __syncthreads();
+  for (uint64_t t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
+    const tile_geom g = tile_of(a, t);
+    tile_setup(a, g, MODE == kRowFilter ? a.rd : nullptr, sm);
     __syncthreads();
-    const OffT *R_t = Rs[buf] + (g.v0 - g.r_al);          // R_t[j] = R[v0 + j]
-    const uint32_t *C_t = Cs[buf] + (g.e_lo - g.e_al);    // C_t[k] = C[e_lo + k]
-    const uint32_t *E_t = Es[buf] + (g.e_lo - g.e_al);
-    // This thread's items [x0, x1) of the merged sequence.
-    const uint64_t x0 = g.item_lo + (uint64_t)tid * kItemsPerThread;
-    const uint64_t x1 = min(x0 + (uint64_t)kItemsPerThread, g.item_hi);
-    uint32_t row = 0;  // local row holding item x0: largest j with v0+j+R[v0+j] <= x0
-    if (x0 < x1) {
-      uint32_t lo = 0, hi = rows;  // answer in [0, rows)
-      while (hi - lo > 1) {
-        const uint32_t mid = (lo + hi) >> 1;
-        if (g.v0 + mid + (uint64_t)R_t[mid] <= x0) lo = mid; else hi = mid;
-      }
-      row = lo;
-    }
-    // Walk the items; segments are (row, partial min).
-    uint32_t seg_row = row, first_row = row, p = kInf, first_p = kInf;
-    bool first_open = true, row_on = false;
-    auto row_active = [&](uint32_t j) -> bool {
-      if (MODE == kEdgeFilter) return true;
-      const uint64_t v = g.v0 + j;
-      return (a.rd[v >> 5] >> (v & 31u)) & 1u;
-    };
-    uint32_t cand[kItemsPerThread];
-    uint32_t crow[kItemsPerThread];
+    const window_rows wr(sm);
+    const uint32_t vb = (uint32_t)(g.v0 & 31u);
+    const int64_t ebase = (int64_t)g.item_lo - (int64_t)g.v0 - 1;  // e = ebase + xi - row
+    // Rows and edge indices of the warp's 8 windows, then every load of the
+    // windows before any use: C and E, the changed-source words, V.
+    uint32_t row[kWindows], src[kWindows], wt[kWindows];
+    uint64_t e[kWindows];
+    bool live[kWindows];
 #pragma unroll
-    for (int k = 0; k < kItemsPerThread; ++k) { cand[k] = kInf; crow[k] = 0xFFFFFFFFu; }
-    // Pass 1: issue every gather (independent loads in flight).
-    {
-      uint32_t r = row;
-      row_on = (x0 < x1) && row_active(r);
-#pragma unroll
-      for (int k = 0; k < kItemsPerThread; ++k) {
-        const uint64_t x = x0 + k;
-        if (x >= x1) break;
-        if (r + 1 < rows + 1 && g.v0 + r + 1 + (uint64_t)R_t[r + 1] == x) {
-          ++r;  // vertex item of row r
-          row_on = row_active(r);
-          continue;
+    for (int k = 0; k < kWindows; ++k) {
+      const uint32_t wi = w * kWindows + k;
+      const uint32_t xi = wi * 32 + lane;
+      const uint32_t word = sm.isv[wi];
+      row[k] = kNone;
+      live[k] = false;
+      e[k] = 0;
+      if (xi < g.nloc) {
+        row[k] = wr.pfx[k] + __popc(word & le_mask) - wr.adj;
+        const bool vertex = (word >> lane) & 1u;
+        bool on = true;
+        if (MODE == kRowFilter) {
+          const uint32_t b = vb + row[k];
+          on = (sm.fw[b >> 5] >> (b & 31u)) & 1u;
         }
-        if (x == g.v0 + r + (uint64_t)R_t[r]) continue;  // the start row's own vertex item
-        const uint64_t e = x - (g.v0 + r) - 1;  // global edge index
-        crow[k] = r;
-        if (!row_on) continue;
-        const uint32_t u = C_t[e - g.e_lo];
-        if (u >= a.n_rows || e >= g.e_hi) {  // staged slice out of step: never gather
-          a.ctr->error = 1u;
-          continue;
+        if (!vertex && on) {
+          const int64_t ei = ebase + (int64_t)xi - (int64_t)row[k];
+          if (ei < 0 || ei >= (int64_t)a.m || row[k] >= g.rows) {
+            a.ctr->error = 1u;  // geometry out of step: never index with it
+          } else {
+            e[k] = (uint64_t)ei;
+            live[k] = true;
+          }
         }
-        if (MODE == kEdgeFilter && !((a.U[u >> 5] >> (u & 31u)) & 1u)) continue;
-        const uint32_t w = kW ? E_t[e - g.e_lo] : 0u;
-        cand[k] = nbr_comp<OP>(a.V[u], w);
-        ++n_edges;
       }
     }
-    // Pass 2: fold candidates into row segments.
-    {
+    // PULL_ALL reads E only for edges from a changed source.
+    constexpr bool kEarlyE = kW && MODE == kRowFilter;
 #pragma unroll
-      for (int k = 0; k < kItemsPerThread; ++k) {
-        if (crow[k] == 0xFFFFFFFFu) continue;
-        if (crow[k] != seg_row) {
-          if (first_open) { first_p = p; first_row = seg_row; first_open = false; }
-          else if (p != kInf) acc_s[seg_row] = p;  // interior row: only writer
-          seg_row = crow[k];
-          p = kInf;
-        }
-        p = min(p, cand[k]);
+    for (int k = 0; k < kWindows; ++k) {
+      src[k] = live[k] ? __ldcs(a.C + e[k]) : 0u;
+      wt[k] = (kEarlyE && live[k]) ? __ldcs(a.E + e[k]) : 0u;
+    }
+#pragma unroll
+    for (int k = 0; k < kWindows; ++k)
+      if (live[k] && src[k] >= a.n_rows) {
+        a.ctr->error = 1u;
+        live[k] = false;
       }
+    if (MODE == kEdgeFilter) {
+      uint32_t uw[kWindows];
+#pragma unroll
+      for (int k = 0; k < kWindows; ++k) uw[k] = live[k] ? a.U[src[k] >> 5] : 0u;
+#pragma unroll
+      for (int k = 0; k < kWindows; ++k)
+        live[k] = live[k] && ((uw[k] >> (src[k] & 31u)) & 1u);
     }
-    // Thread-boundary segments: first (and last, if different) via warp runs.
-    uint32_t fr = 0xFFFFFFFFu, fp = kInf, lr = 0xFFFFFFFFu, lp = kInf;
-    if (x0 < x1) {
-      if (first_open) { fr = seg_row; fp = p; }
-      else { fr = first_row; fp = first_p; lr = seg_row; lp = p; }
+    uint32_t val[kWindows];
+#pragma unroll
+    for (int k = 0; k < kWindows; ++k) {
+      if (kW && !kEarlyE) wt[k] = live[k] ? __ldcs(a.E + e[k]) : 0u;
+      val[k] = live[k] ? a.V[src[k]] : kInf;
     }
-    {
+#pragma unroll
+    for (int k = 0; k < kWindows; ++k) {
+      const uint32_t cand = live[k] ? nbr_comp<OP>(val[k], wt[k]) : kInf;
+      n_edges += live[k] ? 1u : 0u;
       bool head;
-      const uint32_t rm = run_mask(fr, &head);
-      const uint32_t q = __reduce_min_sync(rm, fp);
-      if (head && fr != 0xFFFFFFFFu && q != kInf) atomicMin(acc_s + fr, q);
-    }
-    {
-      bool head;
-      const uint32_t rm = run_mask(lr, &head);
-      const uint32_t q = __reduce_min_sync(rm, lp);
-      if (head && lr != 0xFFFFFFFFu && q != kInf) atomicMin(acc_s + lr, q);
+      const uint32_t rm = run_mask(row[k], &head);
+      const uint32_t q = __reduce_min_sync(rm, cand);
+      if (head && q != kInf) atomicMin(&sm.acc[row[k]], q);
     }
     __syncthreads();
-    // Finalise the tile's rows.
-    for (uint32_t jb = 0; jb < rows; jb += kSweepThreads) {
+    // Finalise the tile's rows.  A row whose items all lie in the tile has
+    // this CTA as its only writer; a split row merges with atomicMin.
+    if (tid < kTileWords) sm.isv[tid] = 0u;  // ready for the next tile
+    for (uint32_t jb = 0; jb < g.rows; jb += kSweepThreads) {
       const uint32_t j = jb + tid;
       bool upd = false;
-      uint64_t v = g.v0 + j;
-      if (j < rows) {
-        const uint32_t acc = acc_s[j];
+      if (j < g.rows) {
+        const uint32_t acc = sm.acc[j];
+        const int32_t p0 = sm.pos[j];
         if (acc != kInf) {
-          const int64_t r0 = (int64_t)R_t[j], r1 = (int64_t)R_t[j + 1];
-          const bool whole = (int64_t)g.item_lo <= (int64_t)v + r0 &&
-                             (int64_t)v + r1 < (int64_t)g.item_hi;
+          const uint64_t v = g.v0 + j;
+          const bool whole = p0 >= 0 && sm.pos[j + 1] <= (int32_t)g.nloc;
           const uint32_t old = a.V[v];
           if (acc < old) upd = whole ? (a.V[v] = acc, true) : (acc < atomicMin(a.V + v, acc));
+        }
+        if (MODE == kRowFilter) {
+          const uint32_t b = vb + j;
+          if ((sm.fw[b >> 5] >> (b & 31u)) & 1u)
+            n_act += (p0 >= 0 && p0 < (int32_t)g.nloc) ? 1u : 0u;
         }
       }
       // Vertices of 32 consecutive rows share at most two words; the second
       // word is touched only when it receives bits (of vertices < n).
-      const uint32_t bit = upd ? 1u : 0u;
-      const uint64_t w0 = (g.v0 + jb + (tid & ~31u)) >> 5;
-      const uint32_t off = (uint32_t)((g.v0 + jb + (tid & ~31u)) & 31u);
-      const uint32_t bal = __ballot_sync(kFull, bit);
+      const uint64_t wv = g.v0 + jb + (tid & ~31u);
+      const uint32_t off = (uint32_t)(wv & 31u);
+      const uint32_t bal = __ballot_sync(kFull, upd);
       if (bal && lane == 0) {
         const uint32_t lo = bal << off, hi = off ? (bal >> (32u - off)) : 0u;
-        if (lo) n_chg += __popc(lo & ~atomicOr(a.chg + w0, lo));
-        if (hi) n_chg += __popc(hi & ~atomicOr(a.chg + w0 + 1, hi));
+        if (lo) n_chg += __popc(lo & ~atomicOr(a.chg + (wv >> 5), lo));
+        if (hi) n_chg += __popc(hi & ~atomicOr(a.chg + (wv >> 5) + 1, hi));
         a.ctr->update_flag = 1u;
-      }
-      if (j < rows && MODE == kRowFilter && row_active(j)) {
-        const int64_t vp = (int64_t)v + (int64_t)R_t[j];
-        n_act += (vp >= (int64_t)g.item_lo && vp < (int64_t)g.item_hi) ? 1u : 0u;
       }
     }
     __syncthreads();
   }
-  cp_async_wait<0>();
   n_act = __reduce_add_sync(kFull, n_act);
   n_edges = __reduce_add_sync(kFull, n_edges);
   n_chg = __reduce_add_sync(kFull, n_chg);
@@ -273,81 +250,70 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(sweep_args<OffT> a) {
   }
 }
 
-// Dense activation: the same staged tiles over the activation adjacency
-// (rows = changed candidates, C = targets); every edge of a row whose bit is
-// set in chg ORs its target's bit into wr.  gate: 2 = run only when the
-// activation is dense (see pull_args), 1 = only when sparse, 0 = always.
+// Dense activation: the same walk over the activation adjacency (rows =
+// changed candidates, C = targets); every edge of a row whose bit is set in
+// rd (the changed rows) ORs its target's bit into chg (the frontier being
+// written), lanes hitting one word in a window combining their bits first.
+// gate: 2 = run only when the changed set is dense (see expand_args).
 template <typename OffT>
 __global__ void __launch_bounds__(kSweepThreads) k_expand_sweep(sweep_args<OffT> a) {
   if (a.ctr->done) return;
   if (a.gate == 2 && !changed_dense(a.ctr, a.gate_cur, a.dense_edges)) return;
-  // Here rd = the changed rows, chg = the frontier being written.
-  extern __shared__ __align__(16) unsigned char smem[];
-  const uint32_t rwords = (kTileItems + 8) * sizeof(OffT) / 4;
-  uint32_t *base = reinterpret_cast<uint32_t *>(smem);
-  OffT *Rs[2];
-  uint32_t *Cs[2];
-  for (int b = 0; b < 2; ++b) {
-    uint32_t *p = base + b * (rwords + 2 * kStageWords);
-    Rs[b] = reinterpret_cast<OffT *>(p);
-    Cs[b] = p + rwords;
-  }
-  const uint32_t tid = threadIdx.x, lane = lane_id();
+  constexpr uint32_t kNone = 0xFFFFFFFFu;
+  __shared__ sweep_smem sm;
+  const uint32_t tid = threadIdx.x, lane = lane_id(), w = tid >> 5;
+  const uint32_t le_mask = kFull >> (31u - lane);
   uint32_t n_rows = 0, n_edges = 0;
-  const uint64_t stride = gridDim.x;
-  uint64_t t = blockIdx.x;
-  if (t < a.ntiles) stage_tile<OffT, false>(a, tile_of(a, t), Rs[0], Cs[0], nullptr);
-  cp_async_commit();
-  int buf = 0;
-  for (; t < a.ntiles; t += stride, buf ^= 1) {
-    const tile_geom<OffT> g = tile_of(a, t);
-    const uint64_t tn = t + stride;
-    if (tn < a.ntiles) stage_tile<OffT, false>(a, tile_of(a, tn), Rs[buf ^ 1], Cs[buf ^ 1], nullptr);
-    cp_async_commit();
-    cp_async_wait<1>();
+  if (tid < kTileWords) sm.isv[tid] = 0u;
+  __syncthreads();
+  for (uint64_t t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
+    const tile_geom g = tile_of(a, t);
+    tile_setup(a, g, a.rd, sm);
     __syncthreads();
-    const uint32_t rows = (uint32_t)(g.v1 - g.v0 + 1);
-    const OffT *R_t = Rs[buf] + (g.v0 - g.r_al);
-    const uint32_t *C_t = Cs[buf] + (g.e_lo - g.e_al);
-    const uint64_t x0 = g.item_lo + (uint64_t)tid * kItemsPerThread;
-    const uint64_t x1 = min(x0 + (uint64_t)kItemsPerThread, g.item_hi);
-    if (x0 < x1) {
-      uint32_t lo = 0, hi = rows;
-      while (hi - lo > 1) {
-        const uint32_t mid = (lo + hi) >> 1;
-        if (g.v0 + mid + (uint64_t)R_t[mid] <= x0) lo = mid; else hi = mid;
-      }
-      uint32_t r = lo;
-      bool on = (a.rd[(g.v0 + r) >> 5] >> ((g.v0 + r) & 31u)) & 1u;
+    const window_rows wr(sm);
+    const uint32_t vb = (uint32_t)(g.v0 & 31u);
+    const int64_t ebase = (int64_t)g.item_lo - (int64_t)g.v0 - 1;
+    uint32_t tgt[kWindows];
 #pragma unroll
-      for (int k = 0; k < kItemsPerThread; ++k) {
-        const uint64_t x = x0 + k;
-        if (x >= x1) break;
-        if (r + 1 <= rows && g.v0 + r + 1 + (uint64_t)R_t[r + 1] == x) {
-          ++r;
-          const uint64_t v = g.v0 + r;
-          on = (a.rd[v >> 5] >> (v & 31u)) & 1u;
-          n_rows += on ? 1u : 0u;
-          continue;
-        }
-        if (x == g.v0 + r + (uint64_t)R_t[r]) {  // the start row's own vertex item
-          n_rows += on ? 1u : 0u;
-          continue;
-        }
-        if (!on) continue;
-        const uint64_t e = x - (g.v0 + r) - 1;
-        const uint32_t tgt = C_t[e - g.e_lo];
-        if (tgt >= a.n_rows || e >= g.e_hi) {  // staged slice out of step
-          a.ctr->error = 1u;
-          continue;
-        }
-        atomicOr(a.chg + (tgt >> 5), 1u << (tgt & 31u));
-        ++n_edges;
+    for (int k = 0; k < kWindows; ++k) {
+      const uint32_t wi = w * kWindows + k;
+      const uint32_t xi = wi * 32 + lane;
+      const uint32_t word = sm.isv[wi];
+      tgt[k] = kNone;
+      if (xi >= g.nloc) continue;
+      const uint32_t r = wr.pfx[k] + __popc(word & le_mask) - wr.adj;
+      const uint32_t b = vb + r;
+      const bool on = r < g.rows && ((sm.fw[b >> 5] >> (b & 31u)) & 1u);
+      if ((word >> lane) & 1u) {
+        n_rows += on ? 1u : 0u;
+        continue;
       }
+      if (!on) continue;
+      const int64_t ei = ebase + (int64_t)xi - (int64_t)r;
+      if (ei < 0 || ei >= (int64_t)a.m) {
+        a.ctr->error = 1u;
+        continue;
+      }
+      tgt[k] = __ldcs(a.C + ei);
+    }
+#pragma unroll
+    for (int k = 0; k < kWindows; ++k) {
+      if (tgt[k] != kNone && tgt[k] >= a.n_rows) {
+        a.ctr->error = 1u;
+        tgt[k] = kNone;
+      }
+      const uint32_t tword = tgt[k] == kNone ? kNone : (tgt[k] >> 5);
+      const uint32_t tbit = tgt[k] == kNone ? 0u : (1u << (tgt[k] & 31u));
+      bool head;
+      const uint32_t rm = run_mask(tword, &head);
+      const uint32_t bits = __reduce_or_sync(rm, tbit);
+      if (head && tword != kNone) atomicOr(a.chg + tword, bits);
+      n_edges += tgt[k] != kNone ? 1u : 0u;
     }
     __syncthreads();
+    if (tid < kTileWords) sm.isv[tid] = 0u;
+    __syncthreads();
   }
-  cp_async_wait<0>();
   n_rows = __reduce_add_sync(kFull, n_rows);
   n_edges = __reduce_add_sync(kFull, n_edges);
   if (lane == 0) {
@@ -356,10 +322,10 @@ __global__ void __launch_bounds__(kSweepThreads) k_expand_sweep(sweep_args<OffT>
   }
 }
 
+// Dynamic shared memory of the sweep kernels (all static now).
 template <typename OffT>
 constexpr size_t sweep_smem_bytes() {
-  return (size_t)2 * ((kTileItems + 8) * sizeof(OffT) + 2 * kStageWords * 4) +
-         (size_t)(kTileItems + 1) * 4;
+  return 0;
 }
 
 }  // namespace kites_internal
