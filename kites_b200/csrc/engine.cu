@@ -134,30 +134,6 @@ int upload_offsets(kites_graph *g, const uint64_t *src64, const uint32_t *src32,
   return KITES_OK;
 }
 
-// Every instantiation of the staged sweep needs more than the default 48 KB
-// of dynamic shared memory.
-template <typename OffT>
-int init_sweep_attrs() {
-  static bool done = false;
-  if (done) return KITES_OK;
-  const int bytes = (int)sweep_smem_bytes<OffT>();
-#define KITES_SWEEP_ATTR(OPV, MODE)                                                        \
-  KITES_CUDA_TRY(cudaFuncSetAttribute(k_sweep<OPV, OffT, MODE>,                            \
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, bytes))
-  KITES_SWEEP_ATTR(OP_SSSP, kRowFilter);
-  KITES_SWEEP_ATTR(OP_SSSP_WRAP, kRowFilter);
-  KITES_SWEEP_ATTR(OP_BFS, kRowFilter);
-  KITES_SWEEP_ATTR(OP_CC, kRowFilter);
-  KITES_SWEEP_ATTR(OP_SSSP, kEdgeFilter);
-  KITES_SWEEP_ATTR(OP_SSSP_WRAP, kEdgeFilter);
-  KITES_SWEEP_ATTR(OP_BFS, kEdgeFilter);
-  KITES_SWEEP_ATTR(OP_CC, kEdgeFilter);
-#undef KITES_SWEEP_ATTR
-  KITES_CUDA_TRY(cudaFuncSetAttribute(k_expand_sweep<OffT>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
-  done = true;
-  return KITES_OK;
-}
 
 // Checks offsets and ids on the device before anything traverses them.
 template <typename OffT>
@@ -337,7 +313,6 @@ int upload_typed(kites_graph *g, const kites_csc_view *v) {
 
   // Staged sweep: tile table, shared-memory opt-in, persistent grid.
   if (g->vpg == 1) {
-    KITES_TRY(init_sweep_attrs<OffT>());
     const uint32_t saved = g->chunk_items;
     g->chunk_items = kTileItems;
     const int st = build_chunk_table<OffT>(g, (const OffT *)g->R, g->n, g->m, &g->chunk_tile,
@@ -351,19 +326,6 @@ int upload_typed(kites_graph *g, const kites_csc_view *v) {
     const uint64_t scap = (uint64_t)std::max(per_sm_sweep, 1) * eng->sm_count;
     g->sweep_grid = (int)std::max<uint64_t>(1, std::min<uint64_t>(g->ntiles, scap));
     g->dense_edges = g->m / 16;
-    // Tiles of the activation adjacency (the in-CSC itself when undirected).
-    if (g->dirR == g->R) {
-      g->chunk_tile_dir = g->chunk_tile;
-      g->ntiles_dir = g->ntiles;
-    } else {
-      g->chunk_items = kTileItems;
-      const int st2 = build_chunk_table<OffT>(g, (const OffT *)g->dirR, g->n_dir_rows,
-                                              g->n_dir_edges, &g->chunk_tile_dir,
-                                              &g->ntiles_dir);
-      g->chunk_items = saved;
-      KITES_TRY(st2);
-    }
-    g->expand_sweep_grid = (int)std::max<uint64_t>(1, std::min<uint64_t>(g->ntiles_dir, scap));
     g->dense_rows = g->n / 32;
   }
   return KITES_OK;
@@ -381,25 +343,26 @@ void launch_sweep(kites_graph *g, const uint32_t *rd, const uint32_t *U, uint32_
                             g->eng->stream>>>(a);
 }
 
-// Activation of the changed rows `chg` into `wr` over an adjacency (rows,
-// targets, chunk and tile tables): the chunked kernel for sparse changed
-// sets, the staged sweep for dense ones (tiles given), one of them working.
+// Activation of the changed rows `chg` into `wr`: the chunked push over the
+// activation adjacency (rows, targets, chunk table) while the changed set is
+// sparse; when `dense_pull` (vertex-level bits, vpg == 1) the pull
+// activation over the in-CSC tiles takes dense changed sets.  Both are
+// launched, the gate lets exactly one do the work.
 template <typename OffT>
 void launch_expand(kites_graph *g, const void *aR, const uint32_t *aC, const uint32_t *chunks,
-                   uint64_t nchunks, const uint32_t *tiles, uint64_t ntiles, uint64_t rows,
-                   uint64_t edges, const uint32_t *chg, uint32_t *wr, uint32_t gate_cur,
-                   uint64_t *launches) {
+                   uint64_t nchunks, bool dense_pull, uint64_t rows, uint64_t edges,
+                   const uint32_t *chg, uint32_t *wr, uint32_t gate_cur, uint64_t *launches) {
   cudaStream_t s = g->eng->stream;
-  const bool sweep = tiles != nullptr;
+  const bool sweep = dense_pull && g->chunk_tile != nullptr;
   chunk_geom<OffT> ga{(const OffT *)aR, aC, chunks, nchunks, rows, rows + edges, g->chunk_items};
   expand_args<OffT> ea{ga, chg, wr, g->ctr, sweep ? 1u : 0u, gate_cur, g->dense_rows};
   k_expand_chunked<OffT><<<g->expand_grid, kBlock, 0, s>>>(ea);
   ++*launches;
   if (sweep) {
-    sweep_args<OffT> sa{(const OffT *)aR, aC, nullptr, nullptr, tiles, ntiles, rows,
-                        rows + edges, chg, nullptr, wr, g->ctr, edges, 2u, gate_cur,
+    sweep_args<OffT> sa{(const OffT *)g->R, g->C, nullptr, nullptr, g->chunk_tile, g->ntiles,
+                        g->n, g->n + g->m, nullptr, chg, wr, g->ctr, g->m, 2u, gate_cur,
                         g->dense_rows};
-    k_expand_sweep<OffT><<<g->expand_sweep_grid, kSweepThreads, sweep_smem_bytes<OffT>(), s>>>(sa);
+    k_activate_sweep<OffT><<<g->sweep_grid, kSweepThreads, 0, s>>>(sa);
     ++*launches;
   }
 }
@@ -426,8 +389,8 @@ int launch_iteration(kites_graph *g, int parity, cudaGraphConditionalHandle h,
     ++*launches;
   }
   if (time_pull) KITES_CUDA_TRY(cudaEventRecord(g->eng->kev1, s));
-  launch_expand<OffT>(g, g->dirR, g->dirC, g->chunk_dir, g->nchunks_dir, g->chunk_tile_dir,
-                      g->ntiles_dir, g->n_dir_rows, g->n_dir_edges, g->changed[parity],
+  launch_expand<OffT>(g, g->dirR, g->dirC, g->chunk_dir, g->nchunks_dir, g->vpg == 1,
+                      g->n_dir_rows, g->n_dir_edges, g->changed[parity],
                       g->frontier[parity ^ 1], 1u, launches);
   // Clear the read frontier and the changed bitmap (adjacent words).
   k_clear_words<<<grid_for(2 * g->nwords, 256, 4096), 256, 0, s>>>(g->frontier[parity],
@@ -449,8 +412,6 @@ struct batch_state {
   const uint32_t *actC;
   const uint32_t *act_chunks;
   uint64_t act_nchunks, act_rows, act_edges;
-  const uint32_t *act_tiles;   // staged-sweep tiles of the adjacency, or null
-  uint64_t act_ntiles;
   int grid;
 };
 
@@ -468,8 +429,8 @@ int launch_batch_iteration(kites_graph *g, const batch_state &b, int parity,
   pull_batch_args<OffT> pa{gb, (const uint32_t *)g->E, b.D, rd, chg, g->ctr};
   k_pull_batch<OP, OffT, K><<<b.grid, kBlock, 0, s>>>(pa);
   if (time_pull) KITES_CUDA_TRY(cudaEventRecord(g->eng->kev1, s));
-  launch_expand<OffT>(g, b.actR, b.actC, b.act_chunks, b.act_nchunks, b.act_tiles,
-                      b.act_ntiles, b.act_rows, b.act_edges, chg, wr, 1u, launches);
+  launch_expand<OffT>(g, b.actR, b.actC, b.act_chunks, b.act_nchunks, true, b.act_rows,
+                      b.act_edges, chg, wr, 1u, launches);
   k_clear_words<<<grid_for(2 * b.nwords, 256, 4096), 256, 0, s>>>(rd, 2 * b.nwords);
   iter_record rec{g->rec_active, g->rec_edges, KITES_MAX_RECORDED_ITERS};
   k_loop_check<<<1, 1, 0, s>>>(g->ctr, rec, h, has_handle);
@@ -713,8 +674,8 @@ int launch_strategy(kites_graph *g, const flex_state &f, int strategy, int parit
   const uint64_t nw = g->nwords;
   auto expand = [&]() {
     // U was marked by the previous iteration: its count is last_changed.
-    launch_expand<OffT>(g, g->dirR, g->dirC, g->chunk_dir, g->nchunks_dir, g->chunk_tile_dir,
-                        g->ntiles_dir, g->n_dir_rows, g->n_dir_edges, Ucur, f.A, 0u, launches);
+    launch_expand<OffT>(g, g->dirR, g->dirC, g->chunk_dir, g->nchunks_dir, g->vpg == 1,
+                        g->n_dir_rows, g->n_dir_edges, Ucur, f.A, 0u, launches);
   };
   switch (strategy) {
     case KITES_STRATEGY_PLAIN: {
@@ -736,7 +697,7 @@ int launch_strategy(kites_graph *g, const flex_state &f, int strategy, int parit
       break;
     }
     case KITES_STRATEGY_PULL_ALL: {
-      launch_sweep<OP, OffT, kEdgeFilter>(g, nullptr, Ucur, Unext, 0u, 0u);
+      launch_sweep<OP, OffT, kAllRows>(g, nullptr, nullptr, Unext, 0u, 0u);
       break;
     }
     case KITES_STRATEGY_TPV1:
@@ -1193,16 +1154,12 @@ int prepare_batch(kites_graph *g, uint32_t K, uint32_t items, batch_state *b) {
     b->nwords = g->bnwords;
   }
   // Vertex-level activation adjacency.
-  b->act_tiles = nullptr;
-  b->act_ntiles = 0;
   if (!g->directed) {
     b->actR = g->R; b->actC = g->C; b->act_chunks = g->chunk_in;
     b->act_nchunks = g->nchunks_in; b->act_rows = g->n; b->act_edges = g->m;
-    b->act_tiles = g->chunk_tile; b->act_ntiles = g->ntiles;
   } else if (g->vpg == 1) {
     b->actR = g->dirR; b->actC = g->dirC; b->act_chunks = g->chunk_dir;
     b->act_nchunks = g->nchunks_dir; b->act_rows = g->n; b->act_edges = g->m;
-    b->act_tiles = g->chunk_tile_dir; b->act_ntiles = g->ntiles_dir;
   } else {
     if (!g->chunk_out)
       KITES_TRY(build_chunk_table<OffT>(g, (const OffT *)g->outR, g->n, g->m, &g->chunk_out,

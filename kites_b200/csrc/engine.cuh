@@ -71,9 +71,6 @@ struct kites_graph {
   uint64_t ntiles = 0;
   int sweep_grid = 0;
   unsigned long long dense_edges = 0;   // PLAIN switches to the sweep above this
-  uint32_t *chunk_tile_dir = nullptr;   // tiles of the activation adjacency
-  uint64_t ntiles_dir = 0;
-  int expand_sweep_grid = 0;
   unsigned long long dense_rows = 0;    // activation switches to the sweep above this
 
   // Frontier: [f0 | c0 | f1 | c1], nwords each.

@@ -267,8 +267,8 @@ struct expand_args {
   const uint32_t *chg;     // changed rows
   uint32_t *wr;            // write frontier
   run_counters *ctr;
-  // Gate: 0 always run; 1 only while the changed set is sparse (the staged
-  // k_expand_sweep takes dense ones).  Dense = changed rows (this
+  // Gate: 0 always run; 1 only while the changed set is sparse (the pull
+  // activation k_activate_sweep takes dense ones).  Dense = changed rows (this
   // iteration's when gate_cur, else the previous one's) above dense_rows.
   uint32_t gate, gate_cur;
   unsigned long long dense_rows;

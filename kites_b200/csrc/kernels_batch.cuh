@@ -52,6 +52,10 @@ __device__ __forceinline__ void store_row(uint32_t *p, const uint32_t (&x)[VPL])
   }
 }
 
+// Source rows each lane group keeps in flight: 8 x K/LPE values per lane.
+template <int K>
+constexpr int rows_in_flight() { return K >= 128 ? 4 : 8; }
+
 template <typename OffT>
 struct pull_batch_args {
   chunk_geom<OffT> g;
@@ -67,6 +71,7 @@ __global__ void __launch_bounds__(kBlock)
     k_pull_batch(pull_batch_args<OffT> a) {
   if (a.ctr->done) return;
   using S = batch_shape<K>;
+  constexpr int kRowsInFlight = rows_in_flight<K>();
   const uint32_t lane = lane_id(), wib = threadIdx.x >> 5;
   const uint32_t sub = lane / S::LPE, kl = lane % S::LPE;
   unsigned long long n_act = 0, n_edges = 0, n_chg = 0;
@@ -106,16 +111,27 @@ __global__ void __launch_bounds__(kBlock)
             cC = __ldcs(a.g.C + t);
             if (op_reads_weights<OP>()) cE = __ldcs(a.E + t);
           }
-#pragma unroll 4
-          for (uint32_t jj = 0; jj < ntile; jj += S::EPW) {
-            const uint32_t j = jj + sub;
-            const uint32_t u = __shfl_sync(kFull, cC, j & 31u);
-            const uint32_t w = __shfl_sync(kFull, cE, j & 31u);
-            if (j < ntile) {
-              uint32_t row[S::VPL];
-              load_row<S::VPL>(a.D + (uint64_t)u * K + kl * S::VPL, row);
+          // kRowsInFlight source rows per lane group are loaded before any
+          // is folded.
+          for (uint32_t jj = 0; jj < ntile; jj += S::EPW * kRowsInFlight) {
+            uint32_t row[kRowsInFlight][S::VPL], wq[kRowsInFlight];
 #pragma unroll
-              for (int q = 0; q < S::VPL; ++q) acc[q] = min(acc[q], nbr_comp<OP>(row[q], w));
+            for (int r = 0; r < kRowsInFlight; ++r) {
+              const uint32_t j = jj + r * S::EPW + sub;
+              const uint32_t u = __shfl_sync(kFull, cC, j & 31u);
+              wq[r] = __shfl_sync(kFull, cE, j & 31u);
+              if (j < ntile) {
+                load_row<S::VPL>(a.D + (uint64_t)u * K + kl * S::VPL, row[r]);
+              } else {
+#pragma unroll
+                for (int q = 0; q < S::VPL; ++q) row[r][q] = kInf;
+              }
+            }
+#pragma unroll
+            for (int r = 0; r < kRowsInFlight; ++r) {
+              if (jj + r * S::EPW + sub >= ntile) continue;
+#pragma unroll
+              for (int q = 0; q < S::VPL; ++q) acc[q] = min(acc[q], nbr_comp<OP>(row[r][q], wq[r]));
             }
           }
         }
