@@ -309,6 +309,11 @@ int kites_autotune(kites_engine *eng, kites_graph *g, int op, const uint32_t *so
  * when the activation edges exceed dense_edges, its activation when the
  * changed rows exceed dense_rows (0 = always, UINT64_MAX = never). */
 int kites_graph_set_density(kites_graph *g, uint64_t dense_edges, uint64_t dense_rows);
+/* How kites_sssp_batch fetches the K-wide source rows (no counterpart in the
+ * reference, whose kernels run one source at a time): 1 (default) = TMA
+ * tile::gather4 copies into shared memory when K >= 32, 0 = register loads.
+ * Both give identical results. */
+int kites_graph_set_batch_gather(kites_graph *g, int mode);
 
 /* ---- synthetic graphs (host, deterministic, OpenMP) ------------------ */
 

@@ -38,6 +38,7 @@ EXPORTED = [
     "kites_selector_load", "kites_selector_save", "kites_graph_set_tpv",
     "kites_sssp_multi_seed", "kites_gen_rmat_union", "kites_autotune",
     "kites_graph_set_density", "kites_sssp_noalloc", "kites_graph_from_edges",
+    "kites_graph_set_batch_gather",
 ]
 SELECTOR_FEATURES, SELECTOR_CLASSES, SELECTOR_PARAMS = 12, 4, 1628
 # Parameter layout of the selector MLP (offsets into the 1628 floats).
@@ -164,6 +165,7 @@ def load(path: str = LIB_PATH):
         "kites_sssp_noalloc": (c_int, [vp, vp, vp, u64, vp, vp, u32, u32, vp, vp,
                                        POINTER(c_uint32)]),
         "kites_graph_from_edges": (c_int, [vp, u64, u64, vp, vp, vp, c_int, vp]),
+        "kites_graph_set_batch_gather": (c_int, [vp, c_int]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)
@@ -428,6 +430,9 @@ class Graph:
         _check(load().kites_selector_record(self.engine._h, self._h, op, source, _p(X), _p(T),
                                             capacity, ctypes.byref(n)))
         return X[: n.value], T[: n.value]
+
+    def set_batch_gather(self, mode):
+        _check(load().kites_graph_set_batch_gather(self._h, int(mode)))
 
     def set_tpv(self, strategy):
         _check(load().kites_graph_set_tpv(self._h, strategy))

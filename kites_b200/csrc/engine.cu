@@ -3,6 +3,7 @@
 // vertex programs (host-driven as in kites/device/compute.cuh:57-128, or a
 // CUDA graph with a conditional while node and device-side convergence).
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 #include <stdio.h>
 #include <string.h>
 
@@ -14,6 +15,7 @@
 #include "engine.cuh"
 #include "kernels.cuh"
 #include "kernels_batch.cuh"
+#include "kernels_batch_tma.cuh"
 #include "kernels_pr.cuh"
 #include "kernels_select.cuh"
 #include "kernels_strategy.cuh"
@@ -311,20 +313,23 @@ int upload_typed(kites_graph *g, const kites_csc_view *v) {
   want = (g->nchunks_dir + kWarpsPerBlock - 1) / kWarpsPerBlock;
   g->expand_grid = (int)(want < cap ? (want ? want : 1) : cap);
 
-  // Staged sweep: tile table, shared-memory opt-in, persistent grid.
+  // Edge-parallel dense sweeps: the row of every edge, persistent grid.
   if (g->vpg == 1) {
-    const uint32_t saved = g->chunk_items;
-    g->chunk_items = kTileItems;
-    const int st = build_chunk_table<OffT>(g, (const OffT *)g->R, g->n, g->m, &g->chunk_tile,
-                                           &g->ntiles);
-    g->chunk_items = saved;
-    KITES_TRY(st);
+    if (g->m) {
+      void *p;
+      KITES_TRY(graph_alloc(g, &p, g->m * 4));
+      g->rowid = (uint32_t *)p;
+      k_row_of_edge<OffT><<<grid_for(g->m), 256, 0, eng->stream>>>((const OffT *)g->R, g->n + 1,
+                                                                  g->m, g->rowid);
+      KITES_CUDA_TRY(cudaGetLastError());
+    }
     int per_sm_sweep = 0;
     KITES_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        &per_sm_sweep, k_sweep<OP_SSSP, OffT, kRowFilter>, kSweepThreads,
-        sweep_smem_bytes<OffT>()));
+        &per_sm_sweep, k_sweep<OP_SSSP, OffT, kRowFilter>, kSweepThreads, 0));
     const uint64_t scap = (uint64_t)std::max(per_sm_sweep, 1) * eng->sm_count;
-    g->sweep_grid = (int)std::max<uint64_t>(1, std::min<uint64_t>(g->ntiles, scap));
+    const uint64_t windows = (g->m + kWindowEdges - 1) / kWindowEdges;
+    const uint64_t want_blocks = (windows + kSweepThreads / 32 - 1) / (kSweepThreads / 32);
+    g->sweep_grid = (int)std::max<uint64_t>(1, std::min<uint64_t>(want_blocks, scap));
     g->dense_edges = g->m / 16;
     g->dense_rows = g->n / 32;
   }
@@ -336,11 +341,10 @@ int upload_typed(kites_graph *g, const kites_csc_view *v) {
 template <int OP, typename OffT, int MODE>
 void launch_sweep(kites_graph *g, const uint32_t *rd, const uint32_t *U, uint32_t *chg,
                   uint32_t gate, uint32_t gate_cur) {
-  sweep_args<OffT> a{(const OffT *)g->R, g->C, (const uint32_t *)g->E, (uint32_t *)g->V,
-                     g->chunk_tile, g->ntiles, g->n, g->n + g->m, rd, U, chg, g->ctr, g->m,
+  sweep_args<OffT> a{(const OffT *)g->R, g->C, (const uint32_t *)g->E, g->rowid,
+                     (uint32_t *)g->V, g->m, g->n, rd, U, chg, g->ctr,
                      gate, gate_cur, g->dense_edges};
-  k_sweep<OP, OffT, MODE><<<g->sweep_grid, kSweepThreads, sweep_smem_bytes<OffT>(),
-                            g->eng->stream>>>(a);
+  k_sweep<OP, OffT, MODE><<<g->sweep_grid, kSweepThreads, 0, g->eng->stream>>>(a);
 }
 
 // Activation of the changed rows `chg` into `wr`: the chunked push over the
@@ -353,15 +357,14 @@ void launch_expand(kites_graph *g, const void *aR, const uint32_t *aC, const uin
                    uint64_t nchunks, bool dense_pull, uint64_t rows, uint64_t edges,
                    const uint32_t *chg, uint32_t *wr, uint32_t gate_cur, uint64_t *launches) {
   cudaStream_t s = g->eng->stream;
-  const bool sweep = dense_pull && g->chunk_tile != nullptr;
+  const bool sweep = dense_pull && g->rowid != nullptr;
   chunk_geom<OffT> ga{(const OffT *)aR, aC, chunks, nchunks, rows, rows + edges, g->chunk_items};
   expand_args<OffT> ea{ga, chg, wr, g->ctr, sweep ? 1u : 0u, gate_cur, g->dense_rows};
   k_expand_chunked<OffT><<<g->expand_grid, kBlock, 0, s>>>(ea);
   ++*launches;
   if (sweep) {
-    sweep_args<OffT> sa{(const OffT *)g->R, g->C, nullptr, nullptr, g->chunk_tile, g->ntiles,
-                        g->n, g->n + g->m, nullptr, chg, wr, g->ctr, g->m, 2u, gate_cur,
-                        g->dense_rows};
+    sweep_args<OffT> sa{(const OffT *)g->R, g->C, nullptr, g->rowid, nullptr, g->m, g->n,
+                        nullptr, chg, wr, g->ctr, 2u, gate_cur, g->dense_rows};
     k_activate_sweep<OffT><<<g->sweep_grid, kSweepThreads, 0, s>>>(sa);
     ++*launches;
   }
@@ -378,7 +381,7 @@ int launch_iteration(kites_graph *g, int parity, cudaGraphConditionalHandle h,
   // Sparse frontiers: per-row chunked pull; dense ones (activation edges of
   // the previous iteration above dense_edges): the staged sweep.  Both are
   // launched, the gate lets exactly one do the work.
-  const bool sweep = g->chunk_tile != nullptr;
+  const bool sweep = g->rowid != nullptr;
   pull_args<OffT> pa{gin, (const uint32_t *)g->E, (uint32_t *)g->V,
                      g->frontier[parity], g->changed[parity], g->shift, g->ctr, nullptr,
                      sweep ? 1u : 0u, 0u, g->dense_edges};
@@ -413,6 +416,8 @@ struct batch_state {
   const uint32_t *act_chunks;
   uint64_t act_nchunks, act_rows, act_edges;
   int grid;
+  bool tma;       // TMA row gathers (g->dmap describes D)
+  int tma_grid;
 };
 
 template <int OP, typename OffT, int K>
@@ -426,8 +431,19 @@ int launch_batch_iteration(kites_graph *g, const batch_state &b, int parity,
   if (time_pull) KITES_CUDA_TRY(cudaEventRecord(g->eng->kev0, s));
   chunk_geom<OffT> gb{(const OffT *)g->R, g->C, g->chunk_batch, g->nchunks_batch,
                       g->n, g->n + g->m, g->batch_chunk_items};
-  pull_batch_args<OffT> pa{gb, (const uint32_t *)g->E, b.D, rd, chg, g->ctr};
-  k_pull_batch<OP, OffT, K><<<b.grid, kBlock, 0, s>>>(pa);
+  bool launched = false;
+  if constexpr (K >= 32) {
+    if (b.tma) {
+      tma_batch_args<OffT> ta{gb, (const uint32_t *)g->E, b.D, rd, chg, g->ctr};
+      k_pull_batch_tma<OP, OffT, K><<<b.tma_grid, kTmaWarps * 32,
+                                      tma_batch_smem_bytes<K, OffT>(), s>>>(g->dmap, ta);
+      launched = true;
+    }
+  }
+  if (!launched) {
+    pull_batch_args<OffT> pa{gb, (const uint32_t *)g->E, b.D, rd, chg, g->ctr};
+    k_pull_batch<OP, OffT, K><<<b.grid, kBlock, 0, s>>>(pa);
+  }
   if (time_pull) KITES_CUDA_TRY(cudaEventRecord(g->eng->kev1, s));
   launch_expand<OffT>(g, b.actR, b.actC, b.act_chunks, b.act_nchunks, true, b.act_rows,
                       b.act_edges, chg, wr, 1u, launches);
@@ -1111,6 +1127,45 @@ void drop_batch_loops(kites_graph *g) {
 
 // Buffers and tables of the batched path for K sources with chunk size
 // `items`; reallocating anything the captured loops point at drops them.
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// against the driver library); null when the driver does not provide it.
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static const PFN_cuTensorMapEncodeTiled_v12000 fn = []() {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) !=
+            cudaSuccess ||
+        q != cudaDriverEntryPointSuccess) {
+      cudaGetLastError();
+      return (PFN_cuTensorMapEncodeTiled_v12000) nullptr;
+    }
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }();
+  return fn;
+}
+
+// Describes D (n rows of K uint32) for tile::gather4 copies: box = one whole
+// row (K values, 128 B .. 1 KB), row coordinates are vertex ids.  False when
+// the map cannot be made (the register-load kernel is used then).
+static bool encode_batch_map(kites_graph *g, uint32_t K) {
+  if (g->dmap_ptr == g->batchD && g->dmap_K == K) return true;
+  g->dmap_ptr = nullptr;
+  const auto encode = tensor_map_encoder();
+  if (!encode || K < 32 || K > 256 || g->n >= (1ull << 31)) return false;
+  const cuuint64_t dims[2] = {K, g->n};
+  const cuuint64_t strides[1] = {(cuuint64_t)K * 4};
+  const cuuint32_t box[2] = {K, 1};
+  const cuuint32_t estr[2] = {1, 1};
+  const CUresult r = encode(&g->dmap, CU_TENSOR_MAP_DATA_TYPE_UINT32, 2, g->batchD, dims,
+                            strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                            CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return false;
+  g->dmap_ptr = g->batchD;
+  g->dmap_K = K;
+  return true;
+}
+
 template <typename OffT>
 int prepare_batch(kites_graph *g, uint32_t K, uint32_t items, batch_state *b) {
   kites_engine *eng = g->eng;
@@ -1168,6 +1223,7 @@ int prepare_batch(kites_graph *g, uint32_t K, uint32_t items, batch_state *b) {
     b->act_nchunks = g->nchunks_out; b->act_rows = g->n; b->act_edges = g->m;
   }
   b->D = g->batchD;
+  b->tma = g->batch_gather != 0 && encode_batch_map(g, K);
   return KITES_OK;
 }
 
@@ -1186,6 +1242,21 @@ int run_batch(kites_graph *g, const uint32_t *sources, uint32_t *dist_out,
   const uint64_t cap = (uint64_t)std::max(per_sm, 1) * eng->sm_count;
   const uint64_t want = (g->nchunks_batch + kWarpsPerBlock - 1) / kWarpsPerBlock;
   b.grid = (int)std::max<uint64_t>(1, std::min(want, cap));
+  if constexpr (K >= 32) {
+    if (b.tma) {
+      const int smem = (int)tma_batch_smem_bytes<K, OffT>();
+      KITES_CUDA_TRY(cudaFuncSetAttribute(k_pull_batch_tma<OP, OffT, K>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+      int tma_per_sm = 0;
+      KITES_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+          &tma_per_sm, k_pull_batch_tma<OP, OffT, K>, kTmaWarps * 32, smem));
+      const uint64_t tcap = (uint64_t)std::max(tma_per_sm, 1) * eng->sm_count;
+      const uint64_t twant = (g->nchunks_batch + kTmaWarps - 1) / kTmaWarps;
+      b.tma_grid = (int)std::max<uint64_t>(1, std::min(twant, tcap));
+    }
+  } else {
+    b.tma = false;
+  }
   KITES_CUDA_TRY(cudaMemcpyAsync(g->d_sources, sources, K * 4, cudaMemcpyDefault, s));
   k_fill_u32<<<grid_for(g->n * K), 256, 0, s>>>(b.D, g->n * K, kInf);
   KITES_CUDA_TRY(cudaMemsetAsync(b.bits, 0, 4 * b.nwords * 4, s));
@@ -2048,7 +2119,7 @@ extern "C" int kites_autotune(kites_engine *eng, kites_graph *g, int op, const u
     return KITES_OK;
   };
   // 1. Density thresholds of the plain loop (vpg == 1 graphs have sweeps).
-  if (g->chunk_tile) {
+  if (g->rowid) {
     const unsigned long long e_cands[] = {g->m / 64, g->m / 32, g->m / 16, g->m / 8, g->m / 4};
     const unsigned long long r_cands[] = {g->n / 128, g->n / 64, g->n / 32, g->n / 16, g->n / 8};
     float best = 1e30f;
@@ -2108,6 +2179,17 @@ extern "C" int kites_autotune(kites_engine *eng, kites_graph *g, int op, const u
     out->batch_ms = best;
   }
   out->batch_chunk_items = g->batch_items_req ? g->batch_items_req : 256u;
+  return KITES_OK;
+}
+
+extern "C" int kites_graph_set_batch_gather(kites_graph *g, int mode) {
+  clear_error();
+  if (!g) return fail(KITES_ERR_INVALID, "null graph");
+  if (mode != 0 && mode != 1) return fail(KITES_ERR_INVALID, "batch gather mode is 0 or 1");
+  KITES_TRY(set_device(g->eng));
+  KITES_CUDA_TRY(cudaStreamSynchronize(g->eng->stream));
+  g->batch_gather = mode;
+  drop_batch_loops(g);  // captured loops hold the kernel choice
   return KITES_OK;
 }
 

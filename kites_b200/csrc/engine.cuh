@@ -1,5 +1,6 @@
 // engine.cuh -- engine and device-graph objects behind the C ABI.
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <map>
@@ -66,9 +67,8 @@ struct kites_graph {
   uint32_t *chunk_dir = nullptr;
   uint64_t nchunks_dir = 0;
 
-  // Tiles of the staged dense sweep (kTileItems items each), vpg == 1 only.
-  uint32_t *chunk_tile = nullptr;
-  uint64_t ntiles = 0;
+  // Row of every in-edge, for the edge-parallel dense sweeps (vpg == 1 only).
+  uint32_t *rowid = nullptr;
   int sweep_grid = 0;
   unsigned long long dense_edges = 0;   // PLAIN switches to the sweep above this
   unsigned long long dense_rows = 0;    // activation switches to the sweep above this
@@ -95,6 +95,12 @@ struct kites_graph {
   uint32_t *chunk_out = nullptr;     // vertex-level out-CSR chunks (vpg > 1)
   uint64_t nchunks_out = 0;
   uint32_t *d_sources = nullptr;     // 256 source slots
+  // TMA view of batchD (K-wide rows) for the gather kernel; batch_gather:
+  // 1 = TMA row gathers when K >= 32, 0 = register loads (default).
+  CUtensorMap dmap;
+  const void *dmap_ptr = nullptr;
+  uint32_t dmap_K = 0;
+  int batch_gather = 0;
   uint32_t *queue = nullptr;         // compacted changed queue (PUSH), n slots
   void *sacc = nullptr;              // selector frontier-count accumulators
   uint8_t *rec_sel = nullptr;        // selector class per iteration (device)

@@ -1,44 +1,35 @@
-// kernels_sweep.cuh -- the tiled dense sweep over the CSC.
+// kernels_sweep.cuh -- the dense sweep: edge-parallel passes over the CSC.
 //
-// For iterations where most rows (or most sources) are live, walking the
-// CSC tile by tile beats per-row discovery.  A tile is kTileItems
-// consecutive items of the merged "row, then its in-edges" sequence (row v
-// at item v + R[v], its edge e at v + 1 + e).  A CTA first marks the tile's
-// vertex items in a shared bitmap (one bit per item) and records each row's
-// local position; then each thread takes 8 consecutive items.  An item's row
-// is the number of vertex items up to it (prefix popcounts of the bitmap)
-// and its edge index follows from the row, so a thread needs no search and
-// no walk; it issues the C/E loads and then the V gathers of all 8 items
-// back to back.  Row minima fold in registers along the thread's items; the
-// first and last row of each thread meet over the warp (runs of equal row)
-// and in a shared accumulator; rows that lie wholly in the tile store their
-// value, rows split across tiles merge into V with global atomicMin.
-//
-// Latency: a CTA walks its tiles in sequence, so every dependent round trip
-// to memory inside a tile costs the whole CTA.  The next tile's table
-// entries and first row offsets are fetched while the current tile works,
-// and the old values of the tile's rows are fetched together with its C
-// loads; what remains per tile is C -> V.
+// For iterations where most rows (or most sources) are live, every in-edge
+// is read anyway, so the work is laid out by edge, not by row: each thread
+// takes 8 consecutive edges (two 16-byte loads each of C, E and the per-edge
+// row index `rowid`, built once at upload), all of its V gathers are in
+// flight together, and the rows' minima fold in registers along the
+// thread's edges (rows are sorted, so a row is a run of equal `rowid`).  A
+// row lying inside one thread's 8 edges is finished by that thread; the
+// first and last row of a thread meet their neighbours over the warp (runs
+// of equal row, `__reduce_min_sync`); whatever crosses a warp's 256-edge
+// window merges into V with atomicMin.  A row is written only when its
+// minimum beats the value read before the fold, and atomicMin's return says
+// whether this warp lowered it (the changed bit).  The row index costs 4
+// bytes per edge more than the item-merged walk it replaces and saves
+// almost all of its per-item arithmetic.
 //
 // Modes: kRowFilter -- rows whose frontier bit is set (PLAIN on a dense
-// frontier); kAllRows -- every row over every in-edge (PULL_ALL on a dense
-// changed set, where testing each source's changed bit would cost one more
-// round trip than the gathers it saves; pulling from an unchanged source
-// cannot lower a row, so the fixed point is the same).  k_activate_sweep
-// computes a dense next frontier by pull over the same tiles.
+// frontier; V gathers are issued with the frontier words, so edges of
+// inactive rows cost a gather but no extra round trip); kAllRows -- every
+// row over every in-edge (PULL_ALL on a dense changed set; pulling from an
+// unchanged source cannot lower a row, so the fixed point is the same).
+// k_activate_sweep computes a dense next frontier by pull with the same
+// layout.
 #pragma once
 #include "kernels.cuh"
 
 namespace kites_internal {
 
 constexpr int kSweepThreads = 256;
-constexpr int kSweepWarps = kSweepThreads / 32;
-constexpr int kTileItems = 2048;                              // items per tile
-constexpr int kTileWords = kTileItems / 32;                   // vertex-item bitmap words
-constexpr int kRowSlots = kTileItems + 4;                     // rows + 1 <= 2050
-constexpr int kFrontierWords = 72;                            // bitmap words of <= 2049 rows
-constexpr int kItemsPerThread = kTileItems / kSweepThreads;  // 8
-static_assert(32 % kItemsPerThread == 0, "a thread's items share one bitmap word");
+constexpr int kEdgesPerThread = 8;
+constexpr int kWindowEdges = 32 * kEdgesPerThread;  // edges per warp step
 
 enum { kRowFilter = 0, kAllRows = 1 };
 
@@ -47,280 +38,165 @@ struct sweep_args {
   const OffT *R;
   const uint32_t *C;
   const uint32_t *E;
+  const uint32_t *rowid;     // row of every edge
   uint32_t *V;
-  const uint32_t *tile_v0;   // chunk table with kTileItems items per chunk
-  uint64_t ntiles, n_rows, n_items;
+  uint64_t m, n_rows;
   const uint32_t *rd;        // kRowFilter: frontier bits
   const uint32_t *U;         // k_activate_sweep: the changed set
   uint32_t *chg;             // next changed bits (activation: the frontier written)
   run_counters *ctr;
-  uint64_t m;                // edges
   // Density gate (see pull_args / expand_args): 2 = run only when dense.
   uint32_t gate, gate_cur;
   unsigned long long dense_edges;
 };
 
-// Shared memory of a sweep CTA (static, < 17 KB).
-struct sweep_smem {
-  int32_t pos[kRowSlots];       // local position of row j's vertex item
-  uint32_t acc[kRowSlots];      // row minima
-  uint32_t isv[kTileWords];     // bit i: item i is a vertex item
-  uint32_t fw[kFrontierWords];  // frontier / changed words of the rows
-};
+constexpr uint32_t kNoRow = 0xFFFFFFFFu;
 
-struct tile_geom {
-  uint64_t item_lo, v0;
-  uint32_t rows, nloc;          // rows v0 .. v0 + rows - 1; items [item_lo, item_lo + nloc)
-};
-
-// A tile's table entries (issued early) and, once they are in, the offset
-// R[v0 + threadIdx.x] of the thread's first row (issued before it is used).
-template <typename OffT>
-struct tile_prefetch {
-  uint64_t t;
-  uint32_t v0, v1;
-  OffT r;
-  __device__ __forceinline__ void start(const sweep_args<OffT> &a, uint64_t tile) {
-    t = tile;
-    v0 = v1 = 0;
-    r = 0;
-    if (t < a.ntiles) {
-      v0 = a.tile_v0[t];
-      v1 = a.tile_v0[t + 1];
+// Loads the thread's 8 edges starting at e0 (a multiple of 8): whole 16-byte
+// vectors when they all exist, element by element at the tail (row = kNoRow
+// past m).  `x` receives the rows, `y` the values of `col`.
+__device__ __forceinline__ void load_edges8(const uint32_t *__restrict__ rowid,
+                                            const uint32_t *__restrict__ col, uint64_t e0,
+                                            uint64_t m, uint32_t (&x)[kEdgesPerThread],
+                                            uint32_t (&y)[kEdgesPerThread]) {
+  if (e0 + kEdgesPerThread <= m) {
+    const uint4 r0 = __ldcs(reinterpret_cast<const uint4 *>(rowid + e0));
+    const uint4 r1 = __ldcs(reinterpret_cast<const uint4 *>(rowid + e0 + 4));
+    const uint4 c0 = __ldcs(reinterpret_cast<const uint4 *>(col + e0));
+    const uint4 c1 = __ldcs(reinterpret_cast<const uint4 *>(col + e0 + 4));
+    x[0] = r0.x; x[1] = r0.y; x[2] = r0.z; x[3] = r0.w;
+    x[4] = r1.x; x[5] = r1.y; x[6] = r1.z; x[7] = r1.w;
+    y[0] = c0.x; y[1] = c0.y; y[2] = c0.z; y[3] = c0.w;
+    y[4] = c1.x; y[5] = c1.y; y[6] = c1.z; y[7] = c1.w;
+  } else {
+#pragma unroll
+    for (int k = 0; k < kEdgesPerThread; ++k) {
+      const bool in = e0 + k < m;
+      x[k] = in ? rowid[e0 + k] : kNoRow;
+      y[k] = in ? col[e0 + k] : 0u;
     }
-  }
-  __device__ __forceinline__ uint32_t rows(const sweep_args<OffT> &a) const {
-    return (uint32_t)(min((uint64_t)v1, a.n_rows - 1) - v0 + 1);
-  }
-  __device__ __forceinline__ void fetch_r(const sweep_args<OffT> &a) {
-    if (t < a.ntiles && threadIdx.x <= rows(a)) r = a.R[(uint64_t)v0 + threadIdx.x];
-  }
-  __device__ __forceinline__ tile_geom geom(const sweep_args<OffT> &a) const {
-    tile_geom g;
-    g.item_lo = t * (uint64_t)kTileItems;
-    g.nloc = (uint32_t)(min(g.item_lo + (uint64_t)kTileItems, a.n_items) - g.item_lo);
-    g.v0 = v0;
-    g.rows = rows(a);
-    return g;
-  }
-};
-
-// pos[j] = v0 + j + R[v0 + j] - item_lo for j in [0, rows], clamped to
-// [-1, kTileItems + 1] (outside the tile only "before" and "after" matter:
-// only row 0 starts before it, only row `rows` after it); the bitmap bit of
-// every vertex item inside the tile; acc = `init`; the rows' bitmap words
-// from `bits` (when given).  r_first = R[v0 + threadIdx.x] (prefetched).
-// isv must be zero on entry.
-template <typename OffT>
-__device__ __forceinline__ void tile_setup(const sweep_args<OffT> &a, const tile_geom &g,
-                                           OffT r_first, const uint32_t *bits, uint32_t init,
-                                           sweep_smem &sm) {
-  for (uint32_t j = threadIdx.x; j <= g.rows; j += kSweepThreads) {
-    const OffT rj = j == threadIdx.x ? r_first : a.R[g.v0 + j];
-    const int64_t p = (int64_t)(g.v0 + j) + (int64_t)rj - (int64_t)g.item_lo;
-    sm.pos[j] = (int32_t)max((int64_t)-1, min(p, (int64_t)kTileItems + 1));
-    if (p >= 0 && p < (int64_t)g.nloc) atomicOr(&sm.isv[p >> 5], 1u << (p & 31));
-    if (j < g.rows) sm.acc[j] = init;
-  }
-  if (bits) {
-    const uint32_t nw = ((uint32_t)(g.v0 & 31u) + g.rows + 31u) >> 5;  // <= 66
-    for (uint32_t i = threadIdx.x; i < nw; i += kSweepThreads) sm.fw[i] = bits[(g.v0 >> 5) + i];
   }
 }
 
-// The thread's items: items 8t .. 8t + 7 of the tile, all inside one bitmap
-// word.  The row of an item is the number of vertex items up to and
-// including it, minus 1 when the tile starts with row v0's vertex item;
-// `before` is that count just ahead of the thread's first item (prefix
-// popcounts of the 64 bitmap words, computed by every warp for itself).
-// Edge items address C through a per-tile base: edge e = e_first + xi - row
-// with e_first = item_lo - v0 - 1, read as base[xi - row - 1] with
-// base = item_lo - v0, valid while xi - row - 1 lies in [lo_ok, hi_ok).
-struct thread_items {
-  uint32_t bits;    // bit k: item k of the thread is a vertex item
-  uint32_t before;  // vertex items before the thread's first item, minus adj
-  int64_t base;
-  int32_t lo_ok, hi_ok;
-  __device__ __forceinline__ thread_items(const sweep_smem &sm, const tile_geom &g, uint64_t m) {
-    const uint32_t lane = lane_id(), w = threadIdx.x >> 5;
-    const uint32_t c0 = __popc(sm.isv[lane]), c1 = __popc(sm.isv[lane + 32]);
-    const uint32_t s0 = warp_inclusive_scan(c0), s1 = warp_inclusive_scan(c1);
-    const uint32_t t0 = __shfl_sync(kFull, s0, 31);
-    const uint32_t ex = w < kSweepWarps / 2 ? s0 - c0 : t0 + s1 - c1;  // warp-uniform choice
-    const uint32_t wi = (threadIdx.x * kItemsPerThread) >> 5;         // this thread's word
-    const uint32_t sh = (threadIdx.x * kItemsPerThread) & 31u;
-    const uint32_t word = sm.isv[wi];
-    const uint32_t pfx = __shfl_sync(kFull, ex, wi & 31u);
-    bits = (word >> sh) & ((1u << kItemsPerThread) - 1u);
-    before = pfx + __popc(word & ((1u << sh) - 1u)) - (sm.pos[0] == 0 ? 1u : 0u);
-    base = (int64_t)g.item_lo - (int64_t)g.v0;
-    lo_ok = (int32_t)max(-base, (int64_t)INT32_MIN);
-    hi_ok = (int32_t)min((int64_t)m - base, (int64_t)INT32_MAX);
+__device__ __forceinline__ void load_vals8(const uint32_t *__restrict__ p, uint64_t e0, uint64_t m,
+                                           uint32_t (&y)[kEdgesPerThread]) {
+  if (e0 + kEdgesPerThread <= m) {
+    const uint4 a = __ldcs(reinterpret_cast<const uint4 *>(p + e0));
+    const uint4 b = __ldcs(reinterpret_cast<const uint4 *>(p + e0 + 4));
+    y[0] = a.x; y[1] = a.y; y[2] = a.z; y[3] = a.w;
+    y[4] = b.x; y[5] = b.y; y[6] = b.z; y[7] = b.w;
+  } else {
+#pragma unroll
+    for (int k = 0; k < kEdgesPerThread; ++k) y[k] = e0 + k < m ? p[e0 + k] : 0u;
   }
-};
-
-// Sets the row bits of a warp's 32 consecutive finalised rows (row wv + i
-// for lane i when `on`): they share at most two words of `bits`, the second
-// touched only when it receives bits.  Returns, in every lane, the bits this
-// call set first.
-__device__ __forceinline__ uint32_t mark_rows(uint32_t *bits, uint64_t wv, bool on) {
-  const uint32_t off = (uint32_t)(wv & 31u);
-  const uint32_t bal = __ballot_sync(kFull, on);
-  uint32_t fresh = 0;
-  if (bal && lane_id() == 0) {
-    const uint32_t lo = bal << off, hi = off ? (bal >> (32u - off)) : 0u;
-    if (lo) fresh |= (lo & ~atomicOr(bits + (wv >> 5), lo)) >> off;
-    if (hi) fresh |= (hi & ~atomicOr(bits + (wv >> 5) + 1, hi)) << (32u - off);
-  }
-  return __shfl_sync(kFull, fresh, 0);
 }
 
 template <int OP, typename OffT, int MODE>
-__global__ void __launch_bounds__(kSweepThreads, 4) k_sweep(sweep_args<OffT> a) {
+__global__ void __launch_bounds__(kSweepThreads) k_sweep(sweep_args<OffT> a) {
   if (a.ctr->done) return;
   if (a.gate == 2 && !frontier_dense(a.ctr, a.gate_cur, a.dense_edges)) return;
   constexpr bool kW = op_reads_weights<OP>();
-  constexpr uint32_t kNone = 0xFFFFFFFFu;
-  __shared__ sweep_smem sm;
-  const uint32_t tid = threadIdx.x;
+  const uint32_t lane = lane_id();
   uint32_t n_act = 0, n_edges = 0, n_chg = 0;
-  if (tid < kTileWords) sm.isv[tid] = 0u;
-  tile_prefetch<OffT> cur, nxt;
-  cur.start(a, blockIdx.x);
-  cur.fetch_r(a);
-  __syncthreads();
-  while (cur.t < a.ntiles) {
-    const tile_geom g = cur.geom(a);
-    tile_setup(a, g, cur.r, MODE == kRowFilter ? a.rd : nullptr, kInf, sm);
-    nxt.start(a, cur.t + gridDim.x);
-    __syncthreads();
-    const thread_items ti(sm, g, a.m);
-    const uint32_t vold = tid < g.rows ? a.V[g.v0 + tid] : 0u;  // used when finalising
-    const uint32_t vb = (uint32_t)(g.v0 & 31u);
-    const uint32_t *Cb = a.C + ti.base;
-    const uint32_t *Eb = kW ? a.E + ti.base : nullptr;
-    uint32_t row[kItemsPerThread], src[kItemsPerThread], wt[kItemsPerThread];
-    int32_t ej[kItemsPerThread];
-    {
-      uint32_t cnt = ti.before;
+  bool any_upd = false;
+  const uint64_t warps = (uint64_t)gridDim.x * (kSweepThreads / 32);
+  for (uint64_t win = ((uint64_t)blockIdx.x * kSweepThreads + threadIdx.x) >> 5;
+       win * kWindowEdges < a.m; win += warps) {
+    const uint64_t e0 = win * kWindowEdges + (uint64_t)lane * kEdgesPerThread;
+    uint32_t row[kEdgesPerThread], src[kEdgesPerThread], wt[kEdgesPerThread];
+    load_edges8(a.rowid, a.C, e0, a.m, row, src);
+    if (kW) load_vals8(a.E, e0, a.m, wt);
+    // The row just before the thread's first edge (to spot row starts).
+    uint32_t prev = __shfl_up_sync(kFull, row[kEdgesPerThread - 1], 1);
+    if (lane == 0) prev = e0 > 0 && e0 <= a.m ? a.rowid[e0 - 1] : kNoRow;
+    // Gathers: V[src] of every edge, the frontier words (row filter), and
+    // the current values of the thread's first and last rows.
+    uint32_t val[kEdgesPerThread], fw[kEdgesPerThread];
+    bool live[kEdgesPerThread];
 #pragma unroll
-      for (int k = 0; k < kItemsPerThread; ++k) {
-        const uint32_t xi = tid * kItemsPerThread + k;
-        const bool vertex = (ti.bits >> k) & 1u;
-        cnt += vertex ? 1u : 0u;
-        row[k] = xi < g.nloc ? cnt : kNone;
-        ej[k] = INT32_MIN;  // no edge to read
-        if (xi < g.nloc && !vertex) {
-          bool on = true;
-          if (MODE == kRowFilter) {
-            const uint32_t b = vb + cnt;
-            on = (sm.fw[b >> 5] >> (b & 31u)) & 1u;
-          }
-          const int32_t j = (int32_t)(xi - cnt) - 1;
-          if (j < ti.lo_ok || j >= ti.hi_ok || cnt >= g.rows) a.ctr->error = 1u;  // out of step
-          else if (on) ej[k] = j;
-        }
+    for (int k = 0; k < kEdgesPerThread; ++k) {
+      live[k] = row[k] != kNoRow;
+      if (live[k] && (src[k] >= a.n_rows || row[k] >= a.n_rows)) {
+        a.ctr->error = 1u;  // never index with an id out of range
+        live[k] = false;
+        row[k] = kNoRow;
       }
+      val[k] = live[k] ? a.V[src[k]] : kInf;
+      fw[k] = (MODE == kRowFilter && live[k]) ? a.rd[row[k] >> 5] : kFull;
     }
+    uint32_t r_first = kNoRow, r_last = kNoRow;  // the thread's first and last valid rows
 #pragma unroll
-    for (int k = 0; k < kItemsPerThread; ++k) {
-      const bool live = ej[k] != INT32_MIN;
-      src[k] = live ? __ldcs(Cb + ej[k]) : 0u;
-      wt[k] = (kW && live) ? __ldcs(Eb + ej[k]) : 0u;
-    }
-    nxt.fetch_r(a);
-    uint32_t cand[kItemsPerThread];
+    for (int k = kEdgesPerThread - 1; k >= 0; --k)
+      if (row[k] != kNoRow) r_first = row[k];
 #pragma unroll
-    for (int k = 0; k < kItemsPerThread; ++k) {
-      bool live = ej[k] != INT32_MIN;
-      if (live && src[k] >= a.n_rows) {
-        a.ctr->error = 1u;
-        live = false;
-        ej[k] = INT32_MIN;
-      }
-      cand[k] = live ? a.V[src[k]] : kInf;
-    }
-#pragma unroll
-    for (int k = 0; k < kItemsPerThread; ++k) {
-      const bool live = ej[k] != INT32_MIN;
-      cand[k] = live ? nbr_comp<OP>(cand[k], wt[k]) : kInf;
-      n_edges += live ? 1u : 0u;
-    }
-    // Fold into row segments: rows interior to the thread have this thread
-    // as their only writer; the first and last segments meet over the warp
-    // (runs of equal row) and in shared memory.
-    uint32_t seg = kNone, p = kInf, first_row = kNone, first_p = kInf;
+    for (int k = 0; k < kEdgesPerThread; ++k)
+      if (row[k] != kNoRow) r_last = row[k];
+    const uint32_t old_first = r_first != kNoRow ? a.V[r_first] : 0u;
+    const uint32_t old_last = r_last != kNoRow ? a.V[r_last] : 0u;
+    // Fold along the thread's edges; count row starts of active rows.
+    uint32_t seg = kNoRow, p = kInf, first_row = kNoRow, first_p = kInf;
     bool first_open = true;
+    uint32_t before = prev;
 #pragma unroll
-    for (int k = 0; k < kItemsPerThread; ++k) {
-      if (row[k] == kNone) continue;
+    for (int k = 0; k < kEdgesPerThread; ++k) {
+      const bool on = live[k] && ((fw[k] >> (row[k] & 31u)) & 1u);
+      if (live[k] && row[k] != before && on) ++n_act;
+      before = row[k];
+      const uint32_t cand = on ? nbr_comp<OP>(val[k], wt[k]) : kInf;
+      n_edges += on ? 1u : 0u;
+      if (row[k] == kNoRow) continue;
       if (row[k] != seg) {
-        if (seg != kNone) {
-          if (first_open) { first_row = seg; first_p = p; first_open = false; }
-          else if (p != kInf) sm.acc[seg] = p;
+        if (seg != kNoRow) {
+          if (first_open) {
+            first_row = seg;
+            first_p = p;
+            first_open = false;
+          } else if (p != kInf) {  // a row wholly inside this thread
+            const uint32_t o = atomicMin(a.V + seg, p);
+            if (p < o) {
+              any_upd = true;
+              n_chg += __popc((1u << (seg & 31u)) & ~atomicOr(a.chg + (seg >> 5), 1u << (seg & 31u)));
+            }
+          }
         }
         seg = row[k];
         p = kInf;
       }
-      p = min(p, cand[k]);
+      p = min(p, cand);
     }
-    uint32_t fr = seg, fp = p, lr = kNone, lp = kInf;
-    if (!first_open) { fr = first_row; fp = first_p; lr = seg; lp = p; }
-    {
+    // fr/lr: the thread's first and last rows (r_first / r_last) with their
+    // partial minima; one row only: fr alone.
+    uint32_t fr = seg, fp = p, lr = kNoRow, lp = kInf;
+    if (!first_open) {
+      fr = first_row;
+      fp = first_p;
+      lr = seg;
+      lp = p;
+    }
+    const uint32_t fold = old_first, lold = old_last;
+    // First and last rows of each thread, merged over the warp.
+#pragma unroll
+    for (int side = 0; side < 2; ++side) {
+      const uint32_t r = side ? lr : fr;
+      const uint32_t v = side ? lp : fp;
+      const uint32_t o = side ? lold : fold;
       bool head;
-      const uint32_t rm = run_mask(fr, &head);
-      const uint32_t q = __reduce_min_sync(rm, fp);
-      if (head && fr != kNone && q != kInf) atomicMin(&sm.acc[fr], q);
-    }
-    {
-      bool head;
-      const uint32_t rm = run_mask(lr, &head);
-      const uint32_t q = __reduce_min_sync(rm, lp);
-      if (head && lr != kNone && q != kInf) atomicMin(&sm.acc[lr], q);
-    }
-    __syncthreads();
-    // Finalise the tile's rows.  A row whose items all lie in the tile has
-    // this CTA as its only writer (so its prefetched value is current); a
-    // split row merges with atomicMin.
-    if (tid < kTileWords) sm.isv[tid] = 0u;  // ready for the next tile
-    for (uint32_t jb = 0; jb < g.rows; jb += kSweepThreads) {
-      const uint32_t j = jb + tid;
-      bool upd = false;
-      if (j < g.rows) {
-        const uint32_t acc = sm.acc[j];
-        const int32_t p0 = sm.pos[j];
-        if (acc != kInf) {
-          const uint64_t v = g.v0 + j;
-          const bool whole = p0 >= 0 && sm.pos[j + 1] <= (int32_t)g.nloc;
-          if (whole) {
-            const uint32_t old = jb == 0 ? vold : a.V[v];
-            if (acc < old) {
-              a.V[v] = acc;
-              upd = true;
-            }
-          } else {
-            upd = acc < atomicMin(a.V + v, acc);
-          }
-        }
-        if (MODE == kRowFilter) {
-          const uint32_t b = vb + j;
-          if ((sm.fw[b >> 5] >> (b & 31u)) & 1u)
-            n_act += (p0 >= 0 && p0 < (int32_t)g.nloc) ? 1u : 0u;
+      const uint32_t rm = run_mask(r, &head);
+      const uint32_t q = __reduce_min_sync(rm, v);
+      if (head && r != kNoRow && q < o) {
+        const uint32_t got = atomicMin(a.V + r, q);
+        if (q < got) {
+          any_upd = true;
+          n_chg += __popc((1u << (r & 31u)) & ~atomicOr(a.chg + (r >> 5), 1u << (r & 31u)));
         }
       }
-      const uint32_t fresh = mark_rows(a.chg, g.v0 + jb + (tid & ~31u), upd);
-      if (fresh && lane_id() == 0) {
-        n_chg += __popc(fresh);
-        a.ctr->update_flag = 1u;
-      }
     }
-    __syncthreads();
-    cur = nxt;
   }
+  if (__any_sync(kFull, any_upd) && lane == 0) a.ctr->update_flag = 1u;
   n_act = __reduce_add_sync(kFull, n_act);
   n_edges = __reduce_add_sync(kFull, n_edges);
   n_chg = __reduce_add_sync(kFull, n_chg);
-  if (lane_id() == 0) {
+  if (lane == 0) {
     if (n_act) atomicAdd(&a.ctr->active, (unsigned long long)n_act);
     if (n_edges) atomicAdd(&a.ctr->edges, (unsigned long long)n_edges);
     if (n_chg) atomicAdd(&a.ctr->changed, (unsigned long long)n_chg);
@@ -329,111 +205,74 @@ __global__ void __launch_bounds__(kSweepThreads, 4) k_sweep(sweep_args<OffT> a) 
 
 // Dense activation by pull: vertex v joins the next frontier (chg) iff one
 // of its in-edges comes from a vertex of the changed set U -- exactly the
-// out-neighbours of U, found over the in-CSC tiles with one load of U per
-// in-edge and no atomics per edge (a push expansion pays an atomicOr per
-// out-edge of every changed vertex).  Counts: updated += changed rows (bit
-// set in U, counted by the tile holding the row's vertex item); out_edges +=
-// in-degree of every newly activated row (the edges the next pull reads).
+// out-neighbours of U -- with one load of U per in-edge and an atomicOr per
+// activated row (a push expansion pays an atomicOr per out-edge of every
+// changed vertex).  Counts: updated += changed rows that have in-edges (the
+// thread holding the row's first edge counts it); out_edges += in-degree of
+// every newly activated row (the edges the next pull reads).
 // gate: 2 = run only when the changed set is dense (see expand_args).
 template <typename OffT>
-__global__ void __launch_bounds__(kSweepThreads, 4) k_activate_sweep(sweep_args<OffT> a) {
+__global__ void __launch_bounds__(kSweepThreads) k_activate_sweep(sweep_args<OffT> a) {
   if (a.ctr->done) return;
   if (a.gate == 2 && !changed_dense(a.ctr, a.gate_cur, a.dense_edges)) return;
-  constexpr uint32_t kNone = 0xFFFFFFFFu;
-  __shared__ sweep_smem sm;
-  const uint32_t tid = threadIdx.x, lane = lane_id();
+  const uint32_t lane = lane_id();
   unsigned long long n_rows = 0, n_edges = 0;
-  if (tid < kTileWords) sm.isv[tid] = 0u;
-  tile_prefetch<OffT> cur, nxt;
-  cur.start(a, blockIdx.x);
-  cur.fetch_r(a);
-  __syncthreads();
-  while (cur.t < a.ntiles) {
-    const tile_geom g = cur.geom(a);
-    tile_setup(a, g, cur.r, a.U, 1u, sm);  // acc[j] = 1: not reached
-    nxt.start(a, cur.t + gridDim.x);
-    __syncthreads();
-    const thread_items ti(sm, g, a.m);
-    const uint32_t *Cb = a.C + ti.base;
-    uint32_t row[kItemsPerThread], src[kItemsPerThread];
-    uint32_t cnt = ti.before;
+  const uint64_t warps = (uint64_t)gridDim.x * (kSweepThreads / 32);
+  for (uint64_t win = ((uint64_t)blockIdx.x * kSweepThreads + threadIdx.x) >> 5;
+       win * kWindowEdges < a.m; win += warps) {
+    const uint64_t e0 = win * kWindowEdges + (uint64_t)lane * kEdgesPerThread;
+    uint32_t row[kEdgesPerThread], src[kEdgesPerThread];
+    load_edges8(a.rowid, a.C, e0, a.m, row, src);
+    uint32_t prev = __shfl_up_sync(kFull, row[kEdgesPerThread - 1], 1);
+    if (lane == 0) prev = e0 > 0 && e0 <= a.m ? a.rowid[e0 - 1] : kNoRow;
+    uint32_t uw[kEdgesPerThread], rw[kEdgesPerThread];
 #pragma unroll
-    for (int k = 0; k < kItemsPerThread; ++k) {
-      const uint32_t xi = tid * kItemsPerThread + k;
-      const bool vertex = (ti.bits >> k) & 1u;
-      cnt += vertex ? 1u : 0u;
-      row[k] = kNone;
-      src[k] = kNone;
-      if (xi >= g.nloc || vertex) continue;
-      const int32_t j = (int32_t)(xi - cnt) - 1;
-      if (j < ti.lo_ok || j >= ti.hi_ok || cnt >= g.rows) {
+    for (int k = 0; k < kEdgesPerThread; ++k) {
+      if (row[k] != kNoRow && (src[k] >= a.n_rows || row[k] >= a.n_rows)) {
         a.ctr->error = 1u;
-        continue;
+        row[k] = kNoRow;
       }
-      row[k] = cnt;
-      src[k] = __ldcs(Cb + j);
+      uw[k] = row[k] != kNoRow ? a.U[src[k] >> 5] : 0u;
+      // The row's own changed bit, read at row starts only.
+      const bool start = row[k] != kNoRow && row[k] != (k ? row[k - 1] : prev);
+      rw[k] = start ? a.U[row[k] >> 5] : 0u;
     }
-    nxt.fetch_r(a);
-    uint32_t uw[kItemsPerThread];
-#pragma unroll
-    for (int k = 0; k < kItemsPerThread; ++k) {
-      if (src[k] != kNone && src[k] >= a.n_rows) {
-        a.ctr->error = 1u;
-        src[k] = kNone;
-        row[k] = kNone;
-      }
-      uw[k] = src[k] != kNone ? a.U[src[k] >> 5] : 0u;
-    }
-    // A row is reached if any of its in-edges is: acc[row] = 0.
-    uint32_t seg = kNone, hit = 0, first_row = kNone, first_hit = 0;
+    uint32_t seg = kNoRow, hit = 0, first_row = kNoRow, first_hit = 0;
     bool first_open = true;
+    auto activate = [&](uint32_t r) {
+      const uint32_t bit = 1u << (r & 31u);
+      if (bit & ~atomicOr(a.chg + (r >> 5), bit))
+        n_edges += (unsigned long long)(a.R[r + 1] - a.R[r]);
+    };
 #pragma unroll
-    for (int k = 0; k < kItemsPerThread; ++k) {
-      if (row[k] == kNone) continue;
+    for (int k = 0; k < kEdgesPerThread; ++k) {
+      if (rw[k] && ((rw[k] >> (row[k] & 31u)) & 1u)) ++n_rows;
+      if (row[k] == kNoRow) continue;
       if (row[k] != seg) {
-        if (seg != kNone) {
-          if (first_open) { first_row = seg; first_hit = hit; first_open = false; }
-          else if (hit) sm.acc[seg] = 0u;
+        if (seg != kNoRow) {
+          if (first_open) {
+            first_row = seg;
+            first_hit = hit;
+            first_open = false;
+          } else if (hit) {
+            activate(seg);
+          }
         }
         seg = row[k];
         hit = 0;
       }
       hit |= (uw[k] >> (src[k] & 31u)) & 1u;
     }
-    uint32_t fr = seg, fh = hit, lr = kNone, lh = 0;
+    uint32_t fr = seg, fh = hit, lr = kNoRow, lh = 0;
     if (!first_open) { fr = first_row; fh = first_hit; lr = seg; lh = hit; }
-    {
+#pragma unroll
+    for (int side = 0; side < 2; ++side) {
+      const uint32_t r = side ? lr : fr;
       bool head;
-      const uint32_t rm = run_mask(fr, &head);
-      const uint32_t q = __reduce_or_sync(rm, fh);
-      if (head && fr != kNone && q) sm.acc[fr] = 0u;
+      const uint32_t rm = run_mask(r, &head);
+      const uint32_t q = __reduce_or_sync(rm, side ? lh : fh);
+      if (head && r != kNoRow && q) activate(r);
     }
-    {
-      bool head;
-      const uint32_t rm = run_mask(lr, &head);
-      const uint32_t q = __reduce_or_sync(rm, lh);
-      if (head && lr != kNone && q) sm.acc[lr] = 0u;
-    }
-    __syncthreads();
-    if (tid < kTileWords) sm.isv[tid] = 0u;
-    const uint32_t vb = (uint32_t)(g.v0 & 31u);
-    for (uint32_t jb = 0; jb < g.rows; jb += kSweepThreads) {
-      const uint32_t j = jb + tid;
-      bool on = false;
-      if (j < g.rows) {
-        on = sm.acc[j] == 0u;
-        const int32_t p0 = sm.pos[j];
-        const uint32_t b = vb + j;
-        if (((sm.fw[b >> 5] >> (b & 31u)) & 1u) && p0 >= 0 && p0 < (int32_t)g.nloc) ++n_rows;
-      }
-      const uint32_t fresh = mark_rows(a.chg, g.v0 + jb + (tid & ~31u), on);
-      if ((fresh >> lane) & 1u) {
-        const uint64_t v = g.v0 + j;
-        n_edges += (unsigned long long)(a.R[v + 1] - a.R[v]);
-      }
-    }
-    __syncthreads();
-    cur = nxt;
   }
   n_rows = __reduce_add_sync(kFull, (uint32_t)n_rows);
 #pragma unroll
@@ -442,12 +281,6 @@ __global__ void __launch_bounds__(kSweepThreads, 4) k_activate_sweep(sweep_args<
     if (n_rows) atomicAdd(&a.ctr->updated, n_rows);
     if (n_edges) atomicAdd(&a.ctr->out_edges, n_edges);
   }
-}
-
-// Dynamic shared memory of the sweep kernels (their shared memory is static).
-template <typename OffT>
-constexpr size_t sweep_smem_bytes() {
-  return 0;
 }
 
 }  // namespace kites_internal

@@ -240,6 +240,30 @@ def test_repeated_runs_and_pool_reuse(engine, cfg1_edges):
     assert pool > 0
 
 
+@pytest.mark.parametrize("k", [32, 64, 128, 256])
+@pytest.mark.parametrize("device_loop", [0, 1])
+def test_batch_gather_modes_agree(engine, k, device_loop):
+    """TMA row gathers (default for K >= 32) and register loads give the same
+    V x K distances, run after run, on one graph."""
+    n = 1 << 14
+    s, d, w = capi.gen_rmat(14, 16 << 14, seed=31)
+    R, C, E = capi.csc_from_edges(n, s, d, w)
+    g = capi.Graph(engine, R, C, E)
+    srcs = np.random.default_rng(100 + k).choice(n, size=k, replace=False).astype(np.uint32)
+    o = capi.default_opts(device_loop=device_loop)
+    tma, st = g.sssp_batch(srcs, opts=o)
+    g.set_batch_gather(0)
+    loads, _ = g.sssp_batch(srcs, opts=o)
+    g.set_batch_gather(1)
+    again, _ = g.sssp_batch(srcs, opts=o)
+    np.testing.assert_array_equal(tma, loads)
+    np.testing.assert_array_equal(again, loads)
+    single, _ = g.sssp(int(srcs[k // 2]))
+    np.testing.assert_array_equal(tma[:, k // 2], single)
+    assert st.iterations > 1
+    g.close()
+
+
 @pytest.mark.parametrize("k", [16, 32, 64, 128, 256])
 @pytest.mark.parametrize("op", [capi.OP_SSSP, capi.OP_BFS])
 def test_batched_sources_match_single_source(engine, k, op):
