@@ -61,6 +61,9 @@ def parse():
                          "single: one source at a time through kites_sssp")
     ap.add_argument("--strategy", default="plain", choices=sorted(STRATEGIES),
                     help="per-iteration strategy of --mode single (batch runs plain)")
+    ap.add_argument("--batch-gather", default="loads", choices=["loads", "tma"],
+                    help="how the batched pull fetches source rows: register loads or "
+                         "TMA tile::gather4 copies")
     ap.add_argument("--host-loop", action="store_true",
                     help="iterate from the host instead of the CUDA-graph device loop "
                          "(for kernel profilers)")
@@ -274,7 +277,7 @@ def workload_config(args):
                      f"uint32 weights U[1,255], no self-loops/duplicates",
             "sources_per_step": args.sources, "mode": args.mode,
             "batch": args.batch if args.mode == "batch" else 1,
-            "strategy": args.strategy,
+            "strategy": args.strategy, "batch_gather": args.batch_gather,
             "l2": "inputs larger than L2 (CSC 2.2 GB, distances 4.3 GB vs 126 MB L2)",
             "parallelism": f"replicas{args.gpus}"}
 
@@ -295,6 +298,7 @@ def run_ours(args):
     eng = capi.Engine(local)
     g = capi.Graph(eng, R, C, E)
     del C, E
+    g.set_batch_gather(1 if args.batch_gather == "tma" else 0)
     stream = torch.cuda.ExternalStream(g.device_view().stream, device=device)
     srcs = pick_sources(outdeg, args.sources, args.seed, offset=rank)
     K = args.batch

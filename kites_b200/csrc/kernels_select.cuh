@@ -81,21 +81,21 @@ __global__ void __launch_bounds__(256) k_select(select_args<OffT> a) {
   __shared__ float x[kFeat], h1[kH], h2[kH], out[kClasses];
   unsigned long long c = 0, os = 0, is = 0;
   unsigned int om = 0;
-  for (uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; w < a.nwords;
-       w += (uint64_t)gridDim.x * blockDim.x) {
-    uint32_t bits = a.U[w];
-    c += __popc(bits);
-    while (bits) {
-      const uint32_t b = __ffs(bits) - 1;
-      bits &= bits - 1;
-      const uint64_t v = w * 32 + b;
-      const uint32_t od = a.out_deg[v];
-      os += od;
-      om = max(om, od);
-      is += (unsigned long long)(a.R[v + 1] - a.R[v]);
-    }
-  }
   const uint32_t lane = lane_id(), wid = threadIdx.x >> 5;
+  // A warp per changed-set word, a lane per bit: the degree loads of one
+  // word's vertices are coalesced.
+  const uint64_t nwarps = (uint64_t)gridDim.x * (blockDim.x >> 5);
+  for (uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < a.nwords;
+       w += nwarps) {
+    const uint32_t bits = a.U[w];
+    if (!((bits >> lane) & 1u)) continue;
+    const uint64_t v = w * 32 + lane;
+    const uint32_t od = a.out_deg[v];
+    ++c;
+    os += od;
+    om = max(om, od);
+    is += (unsigned long long)(a.R[v + 1] - a.R[v]);
+  }
   c = __reduce_add_sync(kFull, (uint32_t)c);
   om = __reduce_max_sync(kFull, om);
 #pragma unroll

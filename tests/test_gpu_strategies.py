@@ -171,3 +171,25 @@ def test_plain_sweep_gate_both_paths(engine, dense):
 def test_selector_rejects_bad_sizes(engine):
     with pytest.raises(capi.KitesError):
         engine.selector_load(np.zeros(10, np.float32))
+
+
+def test_default_selector_is_trained_and_exact(cfg1_edges):
+    """A fresh engine carries the trained default selector (compiled in from
+    selector_default.inc), and AUTO with it reaches the oracle's fixed point."""
+    eng = capi.Engine(0)
+    try:
+        P = eng.selector_save()
+        neutral = np.zeros(capi.SELECTOR_PARAMS, np.float32)
+        neutral[capi.SEL_OFF["std"]:capi.SEL_OFF["std"] + 12] = 1.0
+        assert not np.array_equal(P, neutral)
+        n = 1 << 16
+        s, d, w = capi.gen_rmat(16, 16 << 16, seed=8)
+        R, C, E = capi.csc_from_edges(n, s, d, w)
+        g = capi.Graph(eng, R, C, E)
+        plain, _ = g.sssp(5)
+        auto, st = g.sssp(5, opts=capi.default_opts(strategy=capi.STRATEGY_AUTO))
+        np.testing.assert_array_equal(auto, plain)
+        assert sum(st.strategy_hist) == st.iterations
+        g.close()
+    finally:
+        eng.close()
