@@ -66,8 +66,10 @@ struct pull_batch_args {
   run_counters *ctr;
 };
 
+// Four CTAs (32 warps) per SM keep more source rows in flight than fewer,
+// fatter warps; K = 256 rows need the registers of two.
 template <int OP, typename OffT, int K>
-__global__ void __launch_bounds__(kBlock)
+__global__ void __launch_bounds__(kBlock, K >= 256 ? 2 : 4)
     k_pull_batch(pull_batch_args<OffT> a) {
   if (a.ctr->done) return;
   using S = batch_shape<K>;

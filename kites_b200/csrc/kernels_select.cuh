@@ -82,19 +82,27 @@ __global__ void __launch_bounds__(256) k_select(select_args<OffT> a) {
   unsigned long long c = 0, os = 0, is = 0;
   unsigned int om = 0;
   const uint32_t lane = lane_id(), wid = threadIdx.x >> 5;
-  // A warp per changed-set word, a lane per bit: the degree loads of one
-  // word's vertices are coalesced.
+  // A warp reads 32 changed-set words at once (one coalesced load, so an
+  // empty stretch costs one load per 32 words); for each non-empty word a
+  // lane takes one bit, so the degree loads of its vertices are coalesced.
   const uint64_t nwarps = (uint64_t)gridDim.x * (blockDim.x >> 5);
-  for (uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < a.nwords;
-       w += nwarps) {
-    const uint32_t bits = a.U[w];
-    if (!((bits >> lane) & 1u)) continue;
-    const uint64_t v = w * 32 + lane;
-    const uint32_t od = a.out_deg[v];
-    ++c;
-    os += od;
-    om = max(om, od);
-    is += (unsigned long long)(a.R[v + 1] - a.R[v]);
+  for (uint64_t base = (((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32;
+       base < a.nwords; base += nwarps * 32) {
+    const uint64_t wl = base + lane;
+    const uint32_t word = wl < a.nwords ? a.U[wl] : 0u;
+    uint32_t nz = __ballot_sync(kFull, word != 0u);
+    while (nz) {
+      const uint32_t i = __ffs(nz) - 1;
+      nz &= nz - 1;
+      const uint32_t bits = __shfl_sync(kFull, word, i);
+      if (!((bits >> lane) & 1u)) continue;
+      const uint64_t v = (base + i) * 32 + lane;
+      const uint32_t od = a.out_deg[v];
+      ++c;
+      os += od;
+      om = max(om, od);
+      is += (unsigned long long)(a.R[v + 1] - a.R[v]);
+    }
   }
   c = __reduce_add_sync(kFull, (uint32_t)c);
   om = __reduce_max_sync(kFull, om);
