@@ -393,11 +393,14 @@ def run_ours(args):
         k_bytes += pst.pull_kernel_bytes
         k_launch += pst.pull_kernel_launches
     p_ach = k_bytes / (k_ms * 1e-3) / 1e9
+    # DRAM bytes per launch of the batched pull, from the ncu summary of the
+    # same workload (one capture of every launch of a step), when there is one.
     traffic = None
-    prof = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(prof):
-        t = json.load(open(prof))
-        traffic = t.get(f"k_pull_batch_K{K}_rmat{args.scale}")
+    prof = os.path.join(ROOT, "profiles", f"k_pull_batch_K{K}_rmat{args.scale}_traffic.md")
+    if args.mode == "batch" and os.path.exists(prof):
+        import re
+        m = re.search(r"DRAM bytes per launch \(read \+ write, mean\): ([0-9]+)", open(prof).read())
+        traffic = int(m.group(1)) if m else None
     src_note = "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback 6.65 TB/s"
 
     # End to end through the C ABI: every batch's V x K distances copied to

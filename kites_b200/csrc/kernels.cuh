@@ -178,68 +178,93 @@ __device__ __forceinline__ void pull_chunks(const pull_args<OffT> &a) {
   uint32_t *acc_s = s_acc[wib];
   uint32_t n_act = 0, n_edges = 0, n_chg = 0;
   const uint64_t stride = (uint64_t)gridDim.x * kWarpsPerBlock;
-  for (uint64_t ch = (uint64_t)blockIdx.x * kWarpsPerBlock + wib; ch < a.g.nchunks;
-       ch += stride) {
-    const int64_t item_lo = (int64_t)(ch * a.g.chunk_items);
-    const int64_t item_hi =
-        min(item_lo + (int64_t)a.g.chunk_items, (int64_t)a.g.n_items);
-    const uint64_t v_first = a.g.chunk_v0[ch];
-    uint64_t v_last = a.g.chunk_v0[ch + 1];
-    if (v_last >= a.g.n_rows) v_last = a.g.n_rows - 1;
-    for (uint64_t vb = v_first & ~31ull; vb <= v_last; vb += 32) {
-      const uint64_t v = vb + lane;
-      const bool in_range = v >= v_first && v <= v_last;
-      bool active = in_range;
-      if (a.rd) {
-        const uint32_t word = a.rd[(vb >> a.shift) >> 5];
-        active = in_range && ((word >> ((v >> a.shift) & 31u)) & 1u);
-      }
-      if (__ballot_sync(kFull, active) == 0) continue;
-      uint32_t cnt = 0, old = 0;
-      OffT elo = 0;
-      bool whole = false;
-      if (active) {
-        const int64_t r0 = (int64_t)a.g.R[v], r1 = (int64_t)a.g.R[v + 1];
-        const int64_t lo = max(r0, item_lo - (int64_t)v - 1);
-        const int64_t hi = min(r1, item_hi - (int64_t)v - 1);
-        cnt = hi > lo ? (uint32_t)(hi - lo) : 0u;
-        elo = (OffT)lo;
-        whole = (lo == r0) && (hi == r1);
-        const int64_t vpos = (int64_t)v + r0;
-        n_act += (vpos >= item_lo && vpos < item_hi) ? 1u : 0u;
-        n_edges += cnt;
-        if (cnt) old = a.V[v];
-      }
-      const uint32_t incl = warp_inclusive_scan(cnt);
-      const uint32_t total = __shfl_sync(kFull, incl, 31);
-      if (total == 0) continue;
-      rs.ex[lane] = incl - cnt;
-      rs.lo[lane] = elo;
-      acc_s[lane] = kInf;
-      __syncwarp();
-      if (kFiltered)
-        fold_min(rs, total, acc_s, filtered_edges<OP>{a.g.C, a.E, a.V, a.U});
-      else
-        fold_min(rs, total, acc_s, pull_edges<OP>{a.g.C, a.E, a.V});
-      bool upd = false;
-      if (cnt) {
-        const uint32_t acc = acc_s[lane];
-        if (acc < old) {
-          if (whole) {
-            a.V[v] = acc;
-            upd = true;
-          } else {
-            upd = acc < atomicMin(a.V + v, acc);
-          }
+  // Warp gw owns chunks gw, gw + W, gw + 2W, ... (W warps in the grid), 32
+  // of them per round: lane l tests whether the round's l-th chunk has any
+  // frontier bit (a short run of words), and only those chunks are walked --
+  // a sparse frontier costs one round trip per 32 chunks instead of a walk
+  // of every chunk.
+  const uint64_t gw = (uint64_t)blockIdx.x * kWarpsPerBlock + wib;
+  for (uint64_t cbase = gw; cbase < a.g.nchunks; cbase += stride * 32) {
+    bool live_chunk = false;
+    {
+      const uint64_t c = cbase + (uint64_t)lane * stride;
+      if (c < a.g.nchunks) {
+        if (!a.rd) {
+          live_chunk = true;
+        } else {
+          const uint64_t v0 = a.g.chunk_v0[c];
+          uint64_t v1 = a.g.chunk_v0[c + 1];
+          if (v1 >= a.g.n_rows) v1 = a.g.n_rows - 1;
+          for (uint64_t w = (v0 >> a.shift) >> 5; w <= (v1 >> a.shift) >> 5; ++w)
+            if (a.rd[w]) { live_chunk = true; break; }
         }
       }
-      __syncwarp();
-      const uint32_t gbit = upd ? (1u << ((v >> a.shift) & 31u)) : 0u;
-      const uint32_t bits = __reduce_or_sync(kFull, gbit);
-      if (bits && lane == 0) {
-        const uint32_t old = atomicOr(a.chg + ((vb >> a.shift) >> 5), bits);
-        n_chg += __popc(bits & ~old);
-        a.ctr->update_flag = 1u;
+    }
+    uint32_t live_mask = __ballot_sync(kFull, live_chunk);
+    while (live_mask) {
+      const uint64_t ch = cbase + (uint64_t)(__ffs(live_mask) - 1) * stride;
+      live_mask &= live_mask - 1;
+      const int64_t item_lo = (int64_t)(ch * a.g.chunk_items);
+      const int64_t item_hi =
+          min(item_lo + (int64_t)a.g.chunk_items, (int64_t)a.g.n_items);
+      const uint64_t v_first = a.g.chunk_v0[ch];
+      uint64_t v_last = a.g.chunk_v0[ch + 1];
+      if (v_last >= a.g.n_rows) v_last = a.g.n_rows - 1;
+      for (uint64_t vb = v_first & ~31ull; vb <= v_last; vb += 32) {
+        const uint64_t v = vb + lane;
+        const bool in_range = v >= v_first && v <= v_last;
+        bool active = in_range;
+        if (a.rd) {
+          const uint32_t word = a.rd[(vb >> a.shift) >> 5];
+          active = in_range && ((word >> ((v >> a.shift) & 31u)) & 1u);
+        }
+        if (__ballot_sync(kFull, active) == 0) continue;
+        uint32_t cnt = 0, old = 0;
+        OffT elo = 0;
+        bool whole = false;
+        if (active) {
+          const int64_t r0 = (int64_t)a.g.R[v], r1 = (int64_t)a.g.R[v + 1];
+          const int64_t lo = max(r0, item_lo - (int64_t)v - 1);
+          const int64_t hi = min(r1, item_hi - (int64_t)v - 1);
+          cnt = hi > lo ? (uint32_t)(hi - lo) : 0u;
+          elo = (OffT)lo;
+          whole = (lo == r0) && (hi == r1);
+          const int64_t vpos = (int64_t)v + r0;
+          n_act += (vpos >= item_lo && vpos < item_hi) ? 1u : 0u;
+          n_edges += cnt;
+          if (cnt) old = a.V[v];
+        }
+        const uint32_t incl = warp_inclusive_scan(cnt);
+        const uint32_t total = __shfl_sync(kFull, incl, 31);
+        if (total == 0) continue;
+        rs.ex[lane] = incl - cnt;
+        rs.lo[lane] = elo;
+        acc_s[lane] = kInf;
+        __syncwarp();
+        if (kFiltered)
+          fold_min(rs, total, acc_s, filtered_edges<OP>{a.g.C, a.E, a.V, a.U});
+        else
+          fold_min(rs, total, acc_s, pull_edges<OP>{a.g.C, a.E, a.V});
+        bool upd = false;
+        if (cnt) {
+          const uint32_t acc = acc_s[lane];
+          if (acc < old) {
+            if (whole) {
+              a.V[v] = acc;
+              upd = true;
+            } else {
+              upd = acc < atomicMin(a.V + v, acc);
+            }
+          }
+        }
+        __syncwarp();
+        const uint32_t gbit = upd ? (1u << ((v >> a.shift) & 31u)) : 0u;
+        const uint32_t bits = __reduce_or_sync(kFull, gbit);
+        if (bits && lane == 0) {
+          const uint32_t old = atomicOr(a.chg + ((vb >> a.shift) >> 5), bits);
+          n_chg += __popc(bits & ~old);
+          a.ctr->update_flag = 1u;
+        }
       }
     }
   }
