@@ -109,6 +109,85 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(sweep_args<OffT> a) {
     // The row just before the thread's first edge (to spot row starts).
     uint32_t prev = __shfl_up_sync(kFull, row[kEdgesPerThread - 1], 1);
     if (lane == 0) prev = e0 > 0 && e0 <= a.m ? a.rowid[e0 - 1] : kNoRow;
+    // Every window but the last has all of its 8 edges per thread: the fast
+    // path below needs no per-edge validity tests and folds branch-free.
+    if (__all_sync(kFull, e0 + kEdgesPerThread <= a.m)) {
+      uint32_t mx = 0;
+#pragma unroll
+      for (int k = 0; k < kEdgesPerThread; ++k) mx = max(mx, max(row[k], src[k]));
+      const bool bad = mx >= a.n_rows || row[0] > row[kEdgesPerThread - 1];
+      if (bad) a.ctr->error = 1u;  // never index with an id out of range
+      uint32_t val[kEdgesPerThread], fw[kEdgesPerThread];
+      uint32_t w_first = kFull, w_last = kFull;
+      if (MODE == kRowFilter && !bad) {
+        w_first = a.rd[row[0] >> 5];
+        w_last = a.rd[row[kEdgesPerThread - 1] >> 5];
+      }
+#pragma unroll
+      for (int k = 0; k < kEdgesPerThread; ++k) {
+        val[k] = bad ? kInf : a.V[src[k]];
+        if (MODE == kRowFilter) {
+          const uint32_t wd = row[k] >> 5;
+          fw[k] = bad ? 0u
+                      : wd == (row[0] >> 5) ? w_first
+                      : wd == (row[kEdgesPerThread - 1] >> 5) ? w_last
+                                                               : a.rd[wd];
+        } else {
+          fw[k] = bad ? 0u : kFull;
+        }
+      }
+      const uint32_t r0 = bad ? kNoRow : row[0];
+      const uint32_t r7 = bad ? kNoRow : row[kEdgesPerThread - 1];
+      const uint32_t old_first = bad ? 0u : a.V[r0];
+      const uint32_t old_last = bad ? 0u : a.V[r7];
+      uint32_t cand[kEdgesPerThread];
+#pragma unroll
+      for (int k = 0; k < kEdgesPerThread; ++k) {
+        const bool on = (fw[k] >> (row[k] & 31u)) & 1u;
+        cand[k] = on ? nbr_comp<OP>(val[k], wt[k]) : kInf;
+        n_edges += on ? 1u : 0u;
+        if (MODE == kRowFilter) n_act += (on && row[k] != (k ? row[k - 1] : prev)) ? 1u : 0u;
+      }
+      // Runs of equal row: p is the running minimum of the current run.
+      uint32_t p = cand[0], fp = kInf;
+#pragma unroll
+      for (int k = 1; k < kEdgesPerThread; ++k) {
+        const bool same = row[k] == row[k - 1];
+        if (!same && !bad) {
+          if (row[k - 1] == r0) {
+            fp = p;  // the first run ends
+          } else if (p != kInf) {  // a row wholly inside this thread
+            const uint32_t sr = row[k - 1];
+            if (p < atomicMin(a.V + sr, p)) {
+              any_upd = true;
+              n_chg += __popc((1u << (sr & 31u)) & ~atomicOr(a.chg + (sr >> 5), 1u << (sr & 31u)));
+            }
+          }
+        }
+        p = same ? min(p, cand[k]) : cand[k];
+      }
+      uint32_t lr = kNoRow, lp = kInf;
+      if (r7 == r0) fp = p;
+      else { lr = r7; lp = p; }
+#pragma unroll
+      for (int side = 0; side < 2; ++side) {
+        const uint32_t r = side ? lr : r0;
+        const uint32_t v = side ? lp : fp;
+        const uint32_t o = side ? old_last : old_first;
+        bool head;
+        const uint32_t rm = run_mask(r, &head);
+        const uint32_t q = __reduce_min_sync(rm, v);
+        if (head && r != kNoRow && q < o) {
+          const uint32_t got = atomicMin(a.V + r, q);
+          if (q < got) {
+            any_upd = true;
+            n_chg += __popc((1u << (r & 31u)) & ~atomicOr(a.chg + (r >> 5), 1u << (r & 31u)));
+          }
+        }
+      }
+      continue;
+    }
+    // The last window: edges past m (row kNoRow) and every test per edge.
     // Gathers: V[src] of every edge, the frontier words (row filter), and
     // the current values of the thread's first and last rows.
     uint32_t val[kEdgesPerThread], fw[kEdgesPerThread];
@@ -225,6 +304,54 @@ __global__ void __launch_bounds__(kSweepThreads) k_activate_sweep(sweep_args<Off
     load_edges8(a.rowid, a.C, e0, a.m, row, src);
     uint32_t prev = __shfl_up_sync(kFull, row[kEdgesPerThread - 1], 1);
     if (lane == 0) prev = e0 > 0 && e0 <= a.m ? a.rowid[e0 - 1] : kNoRow;
+    auto activate = [&](uint32_t r) {
+      const uint32_t bit = 1u << (r & 31u);
+      if (bit & ~atomicOr(a.chg + (r >> 5), bit))
+        n_edges += (unsigned long long)(a.R[r + 1] - a.R[r]);
+    };
+    // Full windows (all but the last): no per-edge validity tests, runs of
+    // equal row folded with selects.
+    if (__all_sync(kFull, e0 + kEdgesPerThread <= a.m)) {
+      uint32_t mx = 0;
+#pragma unroll
+      for (int k = 0; k < kEdgesPerThread; ++k) mx = max(mx, max(row[k], src[k]));
+      const bool bad = mx >= a.n_rows || row[0] > row[kEdgesPerThread - 1];
+      if (bad) a.ctr->error = 1u;
+      uint32_t hit[kEdgesPerThread];
+#pragma unroll
+      for (int k = 0; k < kEdgesPerThread; ++k) {
+        const uint32_t uw = bad ? 0u : a.U[src[k] >> 5];
+        hit[k] = (uw >> (src[k] & 31u)) & 1u;
+        // The row's own changed bit, read at row starts only.
+        const bool start = !bad && row[k] != (k ? row[k - 1] : prev);
+        const uint32_t rw = start ? a.U[row[k] >> 5] : 0u;
+        n_rows += (rw >> (row[k] & 31u)) & 1u;
+      }
+      const uint32_t r0 = bad ? kNoRow : row[0];
+      const uint32_t r7 = bad ? kNoRow : row[kEdgesPerThread - 1];
+      uint32_t h = hit[0], fh = 0;
+#pragma unroll
+      for (int k = 1; k < kEdgesPerThread; ++k) {
+        const bool same = row[k] == row[k - 1];
+        if (!same && !bad) {
+          if (row[k - 1] == r0) fh = h;
+          else if (h) activate(row[k - 1]);  // a row wholly inside this thread
+        }
+        h = same ? (h | hit[k]) : hit[k];
+      }
+      uint32_t lr = kNoRow, lh = 0;
+      if (r7 == r0) fh = h;
+      else { lr = r7; lh = h; }
+#pragma unroll
+      for (int side = 0; side < 2; ++side) {
+        const uint32_t r = side ? lr : r0;
+        bool head;
+        const uint32_t rm = run_mask(r, &head);
+        const uint32_t q = __reduce_or_sync(rm, side ? lh : fh);
+        if (head && r != kNoRow && q) activate(r);
+      }
+      continue;
+    }
     uint32_t uw[kEdgesPerThread], rw[kEdgesPerThread];
 #pragma unroll
     for (int k = 0; k < kEdgesPerThread; ++k) {
@@ -239,11 +366,6 @@ __global__ void __launch_bounds__(kSweepThreads) k_activate_sweep(sweep_args<Off
     }
     uint32_t seg = kNoRow, hit = 0, first_row = kNoRow, first_hit = 0;
     bool first_open = true;
-    auto activate = [&](uint32_t r) {
-      const uint32_t bit = 1u << (r & 31u);
-      if (bit & ~atomicOr(a.chg + (r >> 5), bit))
-        n_edges += (unsigned long long)(a.R[r + 1] - a.R[r]);
-    };
 #pragma unroll
     for (int k = 0; k < kEdgesPerThread; ++k) {
       if (rw[k] && ((rw[k] >> (row[k] & 31u)) & 1u)) ++n_rows;
