@@ -67,6 +67,9 @@ def parse():
     ap.add_argument("--host-loop", action="store_true",
                     help="iterate from the host instead of the CUDA-graph device loop "
                          "(for kernel profilers)")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="skip kites_autotune (batch chunk size, sweep densities, TPV width) "
+                         "before the warm-up")
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--ref-sample-scale", type=int, default=20)
     ap.add_argument("--no-e2e", action="store_true")
@@ -307,6 +310,12 @@ def run_ours(args):
     groups = [srcs[i:i + K] for i in range(0, len(srcs), K)]
     if args.mode == "batch" and args.strategy != "plain":
         raise SystemExit("--mode batch runs the plain strategy")
+    tuned = None
+    if not args.no_autotune:
+        r = g.autotune(srcs[:8], batch=K if args.mode == "batch" else 16)
+        tuned = {"batch_chunk_items": int(r.batch_chunk_items),
+                 "dense_edges": int(r.dense_edges), "dense_rows": int(r.dense_rows),
+                 "tpv_strategy": int(r.tpv_strategy), "trials": int(r.trials)}
     loop = 0 if args.host_loop else 1
     bopts = capi.default_opts(device_loop=loop)
     sopts = capi.default_opts(device_loop=loop, strategy=STRATEGIES[args.strategy])
@@ -457,7 +466,7 @@ def run_ours(args):
             "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-            "config": workload_config(args),
+            "config": dict(workload_config(args), autotuned=tuned),
             "clocks": clk.summary(),
             "e2e": e2e,
             "gpu_launches": int(launches),

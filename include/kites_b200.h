@@ -94,6 +94,9 @@ typedef struct kites_csc_view {
   const uint32_t *out_col_indices;  /* dir_C                                  */
   uint64_t n_out_edges;
   int32_t on_device;                /* 1 if every pointer above is device memory */
+  int32_t offsets64;                /* 1: keep row offsets in uint64 on the device even
+                                       when uint32 would do (the layout graphs past
+                                       2^32 vertices + edges get) */
 } kites_csc_view;
 
 /* Device pointers of an uploaded graph, for the header-side generic kernels

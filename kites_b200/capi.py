@@ -58,7 +58,7 @@ class CscView(Structure):
         ("frontier_nbits", c_uint64), ("n_out_rows", c_uint64),
         ("out_row_offsets", c_void_p), ("out_row_offsets32", c_void_p),
         ("out_col_indices", c_void_p), ("n_out_edges", c_uint64),
-        ("on_device", c_int32),
+        ("on_device", c_int32), ("offsets64", c_int32),
     ]
 
 
@@ -271,7 +271,7 @@ class Graph:
     def __init__(self, engine: Engine, R, C, E=None, V=None, frontier=None,
                  frontier_nbits=0, vpg=1, directed=True, dir_R=None, dir_C=None,
                  on_device=False, n_vertices=None, n_edges=None,
-                 vertex_value_size=4):
+                 vertex_value_size=4, offsets64=False):
         self.engine = engine
         v = CscView()
         if on_device:
@@ -315,6 +315,7 @@ class Graph:
             v.out_col_indices = _p(dir_C)
             v.n_out_edges = dir_C.shape[0]
         v.on_device = 1 if on_device else 0
+        v.offsets64 = 1 if offsets64 else 0
         self._keep = (R, C, E, V, frontier, dir_R, dir_C)
         self._h = c_void_p()
         _check(load().kites_graph_upload(engine._h, ctypes.byref(v), ctypes.byref(self._h)))

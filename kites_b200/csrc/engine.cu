@@ -1529,7 +1529,7 @@ extern "C" int kites_graph_upload(kites_engine *eng, const kites_csc_view *v,
   g->vpg = vpg;
   while ((1u << g->shift) < vpg) ++g->shift;
   g->directed = v->directed ? 1 : 0;
-  g->off64 = g->m > 0xFFFFFFFFull - g->n;
+  g->off64 = v->offsets64 != 0 || g->m > 0xFFFFFFFFull - g->n;
   g->vsize = v->vertex_value_size ? v->vertex_value_size : 4;
   g->esize = v->edge_value_size;
   int st = g->off64 ? upload_typed<uint64_t>(g, v) : upload_typed<uint32_t>(g, v);

@@ -184,7 +184,11 @@ void kor_pagerank_f64(uint64_t n_real, const uint64_t *R, const uint32_t *C,
     for (uint64_t v = 0; v < n_real; ++v)
         pr[v] = 1.0 / (double)n_real;
     for (uint32_t it = 0; it < iterations; ++it) {
-        for (uint64_t v = 0; v < n_real; ++v) {
+        /* Rows are independent within a Jacobi step and each row sums its
+         * in-edges in CSC order, so the threads change no result. */
+        #pragma omp parallel for schedule(dynamic, 4096)
+        for (int64_t vi = 0; vi < (int64_t)n_real; ++vi) {
+            const uint64_t v = (uint64_t)vi;
             double s = 0.0;
             for (uint64_t e = R[v]; e < R[v + 1]; ++e) {
                 uint32_t u = C[e];

@@ -316,3 +316,47 @@ def test_batch_rejects_bad_input(engine, cfg1_edges):
     assert ei.value.status == capi.ERR_INVALID
     dist, _ = g.sssp_batch(np.arange(16, dtype=np.uint32))  # still usable
     assert dist[0, 0] == 0
+
+
+@pytest.mark.parametrize("offsets64", [0, 1])
+def test_uint64_offsets_give_the_same_results(engine, offsets64):
+    """Graphs past 2^32 vertices + edges keep 64-bit row offsets on the device;
+    a small graph asked for that layout runs every path of the uint64
+    instantiations and must agree bit for bit with the uint32 layout."""
+    n = 1 << 14
+    s, d, w = capi.gen_rmat(14, 16 << 14, seed=17)
+    R, C, E = capi.csc_from_edges(n, s, d, w)
+    g32 = capi.Graph(engine, R, C, E)
+    g = capi.Graph(engine, R, C, E, offsets64=bool(offsets64))
+    assert g.device_view().offsets64 == offsets64
+    for strat in (capi.STRATEGY_PLAIN, capi.STRATEGY_AUTO, capi.STRATEGY_PUSH,
+                  capi.STRATEGY_PULL_ALL, capi.STRATEGY_TPV8):
+        o = capi.default_opts(strategy=strat)
+        np.testing.assert_array_equal(g.sssp(7, opts=o)[0], g32.sssp(7)[0])
+    np.testing.assert_array_equal(g.sssp(7, op=capi.OP_BFS)[0], g32.sssp(7, op=capi.OP_BFS)[0])
+    srcs = np.arange(64, dtype=np.uint32) * 101
+    for mode in (0, 1):
+        g.set_batch_gather(mode)
+        np.testing.assert_array_equal(g.sssp_batch(srcs)[0], g32.sssp_batch(srcs)[0])
+    pr, _ = g.pagerank(n_real=n)
+    pr32, _ = g32.pagerank(n_real=n)
+    assert np.abs(pr.astype(np.float64) - pr32).sum() / np.abs(pr32).sum() < 1e-6
+    V0 = np.full(n, INF, np.uint32)
+    V0[7] = 0
+    want, _ = O.sanity_check(R, C, E, V0, op=O.OP_SSSP_SAT)
+    np.testing.assert_array_equal(g.sssp(7)[0], want)
+    g.close()
+    g32.close()
+
+
+def test_uint64_offsets_undirected_cc(engine, cfg1_edges, golden):
+    s, d, _ = cfg1_edges
+    ss, tt = np.concatenate([s, d]), np.concatenate([d, s])
+    k = np.unique(ss.astype(np.uint64) << np.uint64(32) | tt)
+    ss = (k >> np.uint64(32)).astype(np.uint32)
+    tt = (k & np.uint64(0xFFFFFFFF)).astype(np.uint32)
+    R, C, _ = capi.csc_from_edges(7115, ss, tt)
+    g = capi.Graph(engine, R, C, None, offsets64=True)
+    labels, _ = g.cc()
+    np.testing.assert_array_equal(labels, golden["cfg1_cc"][:7115])
+    g.close()

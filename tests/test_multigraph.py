@@ -59,3 +59,33 @@ def test_multigraph_batch_matches_members(engine, strategy):
     # Full-size certificate over the whole union.
     ok, msg = O.certify_shortest_paths(R, C, E, dist, seeds)
     assert ok, msg
+
+
+@pytest.mark.gpu
+def test_thousand_graph_batch(engine):
+    """The full multi-graph batch: 1,000 independent R-MAT graphs, vertex
+    counts log-uniform in [1K, 100K], edge factors in [4, 32], vertex 0 of
+    every member as its seed, one run of the CUDA-graph device loop with the
+    learned selector.  Every member's distances form its own shortest-path
+    fixed point (certificate over the whole union) and sampled members match
+    the oracle's sequential loop."""
+    s, d, w, vo, eo = capi.gen_rmat_union(1000, seed=11, v_min=1000, v_max=100000)
+    n = int(vo[-1])
+    assert vo.shape[0] == 1001
+    R, C, E = capi.csc_from_edges(n, s, d, w)
+    g = capi.Graph(engine, R, C, E)
+    seeds = vo[:-1].astype(np.uint32)
+    dist, st = g.sssp_multi_seed(seeds, opts=capi.default_opts(strategy=capi.STRATEGY_AUTO))
+    ok, msg = O.certify_shortest_paths(R, C, E, dist, seeds)
+    assert ok, msg
+    plain, _ = g.sssp_multi_seed(seeds)
+    np.testing.assert_array_equal(dist, plain)
+    for i in (0, 499, 999):
+        lo, hi = int(vo[i]), int(vo[i + 1])
+        el, eh = int(eo[i]), int(eo[i + 1])
+        Ri, Ci, Ei = capi.csc_from_edges(hi - lo, s[el:eh] - lo, d[el:eh] - lo, w[el:eh])
+        V0 = np.full(hi - lo, INF, np.uint32)
+        V0[0] = 0
+        want, _ = O.sanity_check(Ri, Ci, Ei, V0, op=O.OP_SSSP_SAT)
+        np.testing.assert_array_equal(dist[lo:hi], want, err_msg=f"member {i}")
+    g.close()
