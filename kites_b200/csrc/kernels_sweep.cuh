@@ -146,7 +146,9 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(sweep_args<OffT> a) {
         const bool on = (fw[k] >> (row[k] & 31u)) & 1u;
         cand[k] = on ? nbr_comp<OP>(val[k], wt[k]) : kInf;
         n_edges += on ? 1u : 0u;
-        if (MODE == kRowFilter) n_act += (on && row[k] != (k ? row[k - 1] : prev)) ? 1u : 0u;
+        // Active rows (row starts in this window), counted in both modes: the
+        // selector's features read them.
+        n_act += (on && row[k] != (k ? row[k - 1] : prev)) ? 1u : 0u;
       }
       // Runs of equal row: p is the running minimum of the current run.
       uint32_t p = cand[0], fp = kInf;
