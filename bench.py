@@ -396,12 +396,18 @@ def run_ours(args):
         b_ach = st.pull_kernel_bytes / (st.pull_kernel_ms * 1e-3) / 1e9
         b_launch = int(st.pull_kernel_launches)
     k_ms, k_bytes, k_launch = 0.0, 0, 0
+    d_ms, d_bytes, d_launch = 0.0, 0, 0
     for s in srcs[:8]:
         _, pst = g.sssp(int(s), out=False, opts=kopts)
         k_ms += pst.pull_kernel_ms
         k_bytes += pst.pull_kernel_bytes
         k_launch += pst.pull_kernel_launches
+        d_ms += pst.pull_dense_ms
+        d_bytes += pst.pull_dense_bytes
+        d_launch += pst.pull_dense_launches
     p_ach = k_bytes / (k_ms * 1e-3) / 1e9
+    # The same restricted to the iterations whose pull ran as the dense sweep.
+    d_ach = d_bytes / (d_ms * 1e-3) / 1e9 if d_ms > 0 else None
     # DRAM bytes per launch of the batched pull, from the ncu summary of the
     # same workload (one capture of every launch of a step), when there is one.
     traffic = None
@@ -486,6 +492,11 @@ def run_ours(args):
                                "kernel": "k_pull_chunked + k_sweep<SSSP> (plain pull phase)",
                                "launches": k_launch,
                                "peak_source": src_note},
+            "roofline_plain_dense": ({"bound": "hbm", "achieved": d_ach, "peak": peak,
+                                      "unit": "GB/s", "frac": d_ach / peak,
+                                      "kernel": "k_sweep<SSSP, row filter> (dense iterations)",
+                                      "launches": d_launch, "peak_source": src_note}
+                                     if d_ach is not None else None),
             "cpu_baseline": cpu,
         }
         print(json.dumps(line))

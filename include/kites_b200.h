@@ -152,6 +152,10 @@ typedef struct kites_run_stats {
   float iter_ms[KITES_MAX_RECORDED_ITERS];
   uint64_t iter_active[KITES_MAX_RECORDED_ITERS];
   uint64_t iter_edges[KITES_MAX_RECORDED_ITERS];
+  double pull_dense_ms;             /* time_kernels, PLAIN: the pulls of the
+                                       iterations the dense sweep ran       */
+  uint64_t pull_dense_launches;
+  uint64_t pull_dense_bytes;        /* algorithmic bytes of those launches   */
 } kites_run_stats;
 
 /* ---- library / engine ------------------------------------------------ */

@@ -93,6 +93,8 @@ class RunStats(Structure):
         ("iter_ms", c_float * MAX_RECORDED_ITERS),
         ("iter_active", c_uint64 * MAX_RECORDED_ITERS),
         ("iter_edges", c_uint64 * MAX_RECORDED_ITERS),
+        ("pull_dense_ms", c_double), ("pull_dense_launches", c_uint64),
+        ("pull_dense_bytes", c_uint64),
     ]
 
 

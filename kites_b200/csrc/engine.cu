@@ -513,6 +513,9 @@ int drive_loop(kites_graph *g, const kites_run_opts &o, loop_key key, Launch lau
     KITES_CUDA_TRY(cudaGraphLaunch(it->second.second, s));
   } else {
     KITES_CUDA_TRY(cudaEventRecord(eng->ev0, s));
+    g->pull_log.clear();
+    // The sweeps' gate reads the previous iteration's activation edges.
+    unsigned long long prev_out_edges = 0;
     for (uint64_t i = 0;; ++i) {
       KITES_TRY(launch((int)(i & 1), 0, 0, launches, o.time_kernels != 0));
       KITES_CUDA_TRY(cudaMemcpyAsync(hctr, g->ctr, sizeof(run_counters),
@@ -523,7 +526,10 @@ int drive_loop(kites_graph *g, const kites_run_opts &o, loop_key key, Launch lau
         KITES_CUDA_TRY(cudaEventElapsedTime(&kms, eng->kev0, eng->kev1));
         st->pull_kernel_ms += kms;
         st->pull_kernel_launches += 1;
+        g->pull_log.push_back({kms, prev_out_edges > g->dense_edges, hctr->last_active,
+                               hctr->last_edges, hctr->total_updated});
       }
+      prev_out_edges = hctr->last_out_edges;
       if (hctr->done) break;
     }
   }
@@ -579,6 +585,21 @@ int run_plain(kites_graph *g, const kites_run_opts &o, kites_run_stats *st) {
       st->pull_kernel_bytes = c.iterations * 4ull * ((g->nbits + 31) / 32) +
                               12ull * c.total_active + (8ull + e_bytes) * c.total_edges +
                               4ull * c.total_updated;
+    if (o.time_kernels && g->rowid) {
+      // The iterations whose pull ran as the dense sweep, alone: the same
+      // algorithmic bytes as above, per iteration.
+      const uint64_t fw = 4ull * ((g->nbits + 31) / 32);
+      unsigned long long upd_before = 0;
+      for (const auto &r : g->pull_log) {
+        if (r.dense) {
+          st->pull_dense_ms += r.ms;
+          st->pull_dense_launches += 1;
+          st->pull_dense_bytes += fw + 12ull * r.active + (8ull + e_bytes) * r.edges +
+                                  4ull * (r.total_updated - upd_before);
+        }
+        upd_before = r.total_updated;
+      }
+    }
     st->kernel_launches += launches;
     if (o.record_iterations) KITES_TRY(record_iterations(g, c, KITES_STRATEGY_PLAIN, st));
   }
@@ -956,6 +977,9 @@ int run_auto(kites_graph *g, const kites_run_opts &o, kites_run_stats *st) {
     KITES_CUDA_TRY(cudaGraphLaunch(ex, s));
   } else {
     KITES_CUDA_TRY(cudaEventRecord(eng->ev0, s));
+    g->pull_log.clear();
+    // The sweeps' gate reads the previous iteration's activation edges.
+    unsigned long long prev_out_edges = 0;
     for (uint64_t i = 0;; ++i) {
       const int parity = (int)(i & 1);
       KITES_TRY(launch_select<OffT>(g, f.U[parity], o.selector_margin, nullptr, 0, 0, 0,
@@ -972,7 +996,10 @@ int run_auto(kites_graph *g, const kites_run_opts &o, kites_run_stats *st) {
         KITES_CUDA_TRY(cudaEventElapsedTime(&kms, eng->kev0, eng->kev1));
         st->pull_kernel_ms += kms;
         st->pull_kernel_launches += 1;
+        g->pull_log.push_back({kms, prev_out_edges > g->dense_edges, hctr->last_active,
+                               hctr->last_edges, hctr->total_updated});
       }
+      prev_out_edges = hctr->last_out_edges;
       if (hctr->done) break;
     }
   }

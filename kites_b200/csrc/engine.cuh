@@ -110,6 +110,15 @@ struct kites_graph {
   // PageRank scratch (allocated on first use).
   float *pr_x = nullptr, *pr_y = nullptr, *pr_inv_out = nullptr;
 
+  // time_kernels: one record per iteration of the last host-loop run (pull
+  // time, whether the dense sweep did the pull, the counters after it).
+  struct pull_rec {
+    float ms;
+    bool dense;
+    unsigned long long active, edges, total_updated;
+  };
+  std::vector<pull_rec> pull_log;
+
   // Instantiated device loops (conditional while graphs), per op/strategy.
   std::map<kites_internal::loop_key, std::pair<cudaGraph_t, cudaGraphExec_t>> loops;
 
