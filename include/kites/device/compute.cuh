@@ -16,6 +16,7 @@
 #include "../../kites_b200.h"
 #include "../common/globals.cuh"
 #include "../graph/graph_csr_device.cuh"
+#include "../graph/graph_csr_mipmapped_device.cuh"
 #include "generic_kernels.cuh"
 #include "nv_gpu.cuh"
 
@@ -68,6 +69,62 @@ void process(graph_csr_device<vT, eT, vIdxT> &g, nv_gpu &dev, FInit fInit, FComp
     CUDAErrorCheck(cudaPeekAtLastError());
     generic::clear_words<<<(unsigned)((nwords + 255) / 256), 256, 0, s>>>(rd, nwords);
     CUDAErrorCheck(cudaMemcpyAsync(hflag, dv.update_flag, sizeof(unsigned),
+                                   cudaMemcpyDeviceToHost, s));
+    ++iterations;
+    CUDAErrorCheck(cudaStreamSynchronize(s));
+  } while (*hflag != 0);
+  const double ms =
+      std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  std::cout << "Processing finished in " << ms << " (ms).\n";
+  std::cout << "Performed " << iterations << " iterations in total.\n";
+}
+
+// Mipmapped graphs: coarse activation (the reference declares the mipmapped
+// graph classes, kites/graph/graph_csr_mipmapped*.{hpp,cuh}, but no process
+// overload consumes them).  The frontier holds one bit per block of
+// compressionRatio vertices; every vertex of an active block pulls with the
+// user functions, and a block with an updated vertex activates every block
+// its mipmap row names.  That activates a superset of the vertices the
+// per-vertex out-adjacency would, so a monotone program (min-plus,
+// min-label, BFS levels) reaches the same fixed point as over graph_csr.
+// Same host loop as above: clear the flag, launch, clear the read frontier,
+// read the flag back.
+template <launch launchMode, class vT, class eT, class vIdxT, class FInit, class FComp,
+          class FRed, class FUpd>
+void process(graph_csr_mipmapped_device<vT, eT, vIdxT> &g, nv_gpu &dev, FInit fInit,
+             FComp fComp, FRed fRed, FUpd fUpd) {
+  dev.setAsActive();
+  const auto mem = dev.queryMemUsage();
+  std::cout << mem.first << " MB is consumed out of the total " << mem.second
+            << " MB global memory.\n";
+  cudaStream_t s = dev.getSsEven().get();
+  const uint64_t n = g.get_num_vertices();
+  const uint32_t words = g.mipmapDim / 32;
+  const unsigned grid = (unsigned)(n / (generic::kWarps * 32));
+  const dim3 egrid((words + 127) / 128,
+                   (g.mipmapDim + generic::kMipRowsPerSlice - 1) / generic::kMipRowsPerSlice);
+  std::cout << "Launching iterative procedure ...\n";
+  auto t0 = std::chrono::steady_clock::now();
+  unsigned iterations = 0;
+  unsigned *hflag = g.updateFlagHost.get_ptr();
+  do {
+    CUDAErrorCheck(cudaMemsetAsync(g.updateFlag.get_ptr(), 0, sizeof(unsigned), s));
+    CUDAErrorCheck(cudaMemsetAsync(g.changedBlocks.get_ptr(), 0, words * sizeof(unsigned), s));
+    const bool even = (iterations & 1) == 0;
+    uint32_t *rd = even ? g.vBitmapEven.get_ptr() : g.vBitmapOdd.get_ptr();
+    uint32_t *wr = even ? g.vBitmapOdd.get_ptr() : g.vBitmapEven.get_ptr();
+    if (grid)
+      generic::mip_pull_iteration<vT, eT><<<grid, generic::kWarps * 32, 0, s>>>(
+          n, g.R.get_ptr(), g.C.get_ptr(), g.V.get_ptr(), g.E.get_ptr(), g.updateFlag.get_ptr(),
+          rd, g.compressionRatio, g.changedBlocks.get_ptr(), fInit, fComp, fRed, fUpd);
+    CUDAErrorCheck(cudaPeekAtLastError());
+    if (words) {
+      generic::mip_expand<<<egrid, 128, 0, s>>>(g.mipmap.get_ptr(), words,
+                                                g.changedBlocks.get_ptr(), wr);
+      CUDAErrorCheck(cudaPeekAtLastError());
+      generic::clear_words<<<(words + 255) / 256, 256, 0, s>>>(rd, words);
+    }
+    CUDAErrorCheck(cudaMemcpyAsync(hflag, g.updateFlag.get_ptr(), sizeof(unsigned),
                                    cudaMemcpyDeviceToHost, s));
     ++iterations;
     CUDAErrorCheck(cudaStreamSynchronize(s));

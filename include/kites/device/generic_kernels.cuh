@@ -43,6 +43,59 @@ __device__ __forceinline__ void run_bounds(uint32_t key, uint32_t lane, uint32_t
   *end = later ? (uint32_t)(__ffs(later) - 2) : 31u;
 }
 
+// The pull of one warp over its 32 consecutive vertices (this lane's vertex
+// v, `active` its frontier test): every active vertex folds its in-edges
+// with the user functions and stores the result when updF accepts it.
+// Returns whether this lane's vertex was updated.  ex/beg/acc/part: the
+// warp's 32-entry rows of shared scratch.
+template <class vT, class eT, class OffT, class FInit, class FComp, class FRed, class FUpd>
+__device__ __forceinline__ bool pull_warp(uint64_t v, bool active, uint32_t lane,
+                                          const OffT *__restrict__ R,
+                                          const uint32_t *__restrict__ C, vT *V, eT *E,
+                                          uint32_t *ex, OffT *beg, vT *acc, vT *part,
+                                          FInit &fInit, FComp &fComp, FRed &fRed, FUpd &fUpd) {
+  uint32_t cnt = 0;
+  vT old{};
+  if (active) {
+    const OffT b = R[v];
+    cnt = (uint32_t)(R[v + 1] - b);
+    beg[lane] = b;
+    old = V[v];
+    vT glob = old;
+    fInit(acc[lane], glob);
+  }
+  const uint32_t incl = scan_incl(cnt, lane);
+  const uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+  ex[lane] = incl - cnt;
+  __syncwarp();
+  for (uint32_t base = 0; base < total; base += 32) {
+    const uint32_t i = base + lane;
+    uint32_t owner = 32u;
+    if (i < total) {
+      uint32_t j = 0;
+#pragma unroll
+      for (uint32_t step = 16; step; step >>= 1)
+        if (ex[j + step] <= i) j += step;
+      owner = j;
+      const OffT e = beg[j] + (OffT)(i - ex[j]);
+      fComp(part[lane], V[C[e]], E + e);
+    }
+    __syncwarp();
+    uint32_t s, t;
+    bool head;
+    run_bounds(owner, lane, &s, &t, &head);
+    if (head && owner < 32u)
+      for (uint32_t k = s; k <= t; ++k) fRed(acc[owner], part[k]);
+    __syncwarp();
+  }
+  bool upd = false;
+  if (active) {
+    upd = fUpd(acc[lane], old);
+    if (upd) V[v] = acc[lane];
+  }
+  return upd;
+}
+
 template <class vT, class eT, class OffT, class FInit, class FComp, class FRed, class FUpd>
 __global__ void __launch_bounds__(kWarps * 32)
     pull_iteration(uint64_t n, const OffT *__restrict__ R, const uint32_t *__restrict__ C,
@@ -62,45 +115,8 @@ __global__ void __launch_bounds__(kWarps * 32)
   const bool active = (word >> ((v >> shift) & 31u)) & 1u;
   if (__ballot_sync(0xFFFFFFFFu, active) == 0) return;
 
-  uint32_t cnt = 0;
-  vT old{};
-  if (active) {
-    const OffT b = R[v];
-    cnt = (uint32_t)(R[v + 1] - b);
-    beg_s[w][lane] = b;
-    old = V[v];
-    vT glob = old;
-    fInit(acc_s[w][lane], glob);
-  }
-  const uint32_t incl = scan_incl(cnt, lane);
-  const uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, 31);
-  ex_s[w][lane] = incl - cnt;
-  __syncwarp();
-  for (uint32_t base = 0; base < total; base += 32) {
-    const uint32_t i = base + lane;
-    uint32_t owner = 32u;
-    if (i < total) {
-      uint32_t j = 0;
-#pragma unroll
-      for (uint32_t step = 16; step; step >>= 1)
-        if (ex_s[w][j + step] <= i) j += step;
-      owner = j;
-      const OffT e = beg_s[w][j] + (OffT)(i - ex_s[w][j]);
-      fComp(part_s[w][lane], V[C[e]], E + e);
-    }
-    __syncwarp();
-    uint32_t s, t;
-    bool head;
-    run_bounds(owner, lane, &s, &t, &head);
-    if (head && owner < 32u)
-      for (uint32_t k = s; k <= t; ++k) fRed(acc_s[w][owner], part_s[w][k]);
-    __syncwarp();
-  }
-  bool upd = false;
-  if (active) {
-    upd = fUpd(acc_s[w][lane], old);
-    if (upd) V[v] = acc_s[w][lane];
-  }
+  const bool upd = pull_warp<vT, eT, OffT>(v, active, lane, R, C, V, E, ex_s[w], beg_s[w],
+                                           acc_s[w], part_s[w], fInit, fComp, fRed, fUpd);
   const uint32_t U = __ballot_sync(0xFFFFFFFFu, upd);
   if (U == 0) return;
   if (lane == 0) *flag = 1u;
@@ -151,6 +167,60 @@ __global__ void __launch_bounds__(kWarps * 32)
     const uint32_t bits = __reduce_or_sync(rm, tb);
     if (head && tw != 0xFFFFFFFFu) atomicOr(wr + tw, bits);
   }
+}
+
+// ---- mipmapped graphs: coarse activation ----------------------------------
+// The frontier holds one bit per block of `cr` consecutive vertices.  Every
+// vertex of an active block pulls; each block with an updated vertex gets
+// its bit in `chg_blocks` (one atomicOr per distinct block per warp).
+template <class vT, class eT, class FInit, class FComp, class FRed, class FUpd>
+__global__ void __launch_bounds__(kWarps * 32)
+    mip_pull_iteration(uint64_t n, const uint32_t *__restrict__ R,
+                       const uint32_t *__restrict__ C, vT *V, eT *E, uint32_t *flag,
+                       const uint32_t *__restrict__ rd, uint32_t cr, uint32_t *chg_blocks,
+                       FInit fInit, FComp fComp, FRed fRed, FUpd fUpd) {
+  __shared__ uint32_t ex_s[kWarps][32];
+  __shared__ uint32_t beg_s[kWarps][32];
+  __shared__ vT acc_s[kWarps][32];
+  __shared__ vT part_s[kWarps][32];
+  const uint32_t lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
+  const uint64_t vb = ((uint64_t)blockIdx.x * kWarps + w) * 32;
+  if (vb >= n) return;  // n is a multiple of 128: whole warps retire
+  const uint64_t v = vb + lane;
+  const uint32_t blk = (uint32_t)(v / cr);
+  const bool active = (rd[blk >> 5] >> (blk & 31u)) & 1u;
+  if (__ballot_sync(0xFFFFFFFFu, active) == 0) return;
+  const bool upd = pull_warp<vT, eT, uint32_t>(v, active, lane, R, C, V, E, ex_s[w], beg_s[w],
+                                               acc_s[w], part_s[w], fInit, fComp, fRed, fUpd);
+  if (__ballot_sync(0xFFFFFFFFu, upd) == 0) return;
+  if (lane == 0) *flag = 1u;
+  const uint32_t peers = __match_any_sync(0xFFFFFFFFu, upd ? blk : 0xFFFFFFFFu);
+  if (upd && (uint32_t)(__ffs(peers) - 1) == lane)
+    atomicOr(chg_blocks + (blk >> 5), 1u << (blk & 31u));
+}
+
+constexpr uint32_t kMipRowsPerSlice = 256;  // block rows per grid row (multiple of 32)
+
+// Next frontier: wr |= OR of the mipmap rows of the changed blocks.  The
+// mipmap is row-major with `words` 32-bit words per row (mipmapDim / 32);
+// a thread owns frontier word j over the kMipRowsPerSlice rows of its grid
+// row, so its loads of row after row are coalesced across the warp.
+__global__ void mip_expand(const uint32_t *__restrict__ mip, uint32_t words,
+                           const uint32_t *__restrict__ chg_blocks, uint32_t *wr) {
+  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= words) return;
+  const uint32_t b0 = blockIdx.y * kMipRowsPerSlice;
+  const uint32_t b1 = min(b0 + kMipRowsPerSlice, words * 32u);
+  uint32_t acc = 0;
+  for (uint32_t b = b0; b < b1; b += 32) {
+    uint32_t bits = chg_blocks[b >> 5];
+    while (bits) {
+      const uint32_t k = __ffs(bits) - 1;
+      bits &= bits - 1;
+      acc |= mip[(uint64_t)(b + k) * words + j];
+    }
+  }
+  if (acc) atomicOr(wr + j, acc);
 }
 
 __global__ void clear_words(uint32_t *p, uint64_t n) {

@@ -1,5 +1,5 @@
 // sanity_check.cuh -- the CPU verifier of the kites:: API (farkhor/KiTES
-// kites/graph/sanity_check.cuh:13-68): a single-thread Gauss-Seidel sweep
+// kites/graph/sanity_check.cuh:13-89): a single-thread Gauss-Seidel sweep
 // over every vertex with the same four functions until nothing changes
 // (the host graph's V becomes that fixed point), then a comparison with the
 // device values.  Prints PASSED or the first mismatch, as the reference does.
@@ -10,6 +10,7 @@
 
 #include "graph_csr.h"
 #include "graph_csr_device.cuh"
+#include "graph_csr_mipmapped_device.cuh"
 
 namespace kites {
 
@@ -54,6 +55,13 @@ bool sanity_check(std::size_t n, host_pinned_buffer<vT> &V, host_pinned_buffer<v
 template <class vT, class eT, class vIdxT, class FInit, class FComp, class FRed, class FUpd>
 bool sanity_check(graph_csr<vT, eT, vIdxT> &h, graph_csr_device<vT, eT, vIdxT> &d, FInit fInit,
                   FComp fComp, FRed fRed, FUpd fUpd) {
+  return sanity_check(h.get_num_vertices(), h.V, h.R, h.C, h.E, d.V, fInit, fComp, fRed, fUpd);
+}
+
+// kites/graph/sanity_check.cuh:82-89
+template <class vT, class eT, class vIdxT, class FInit, class FComp, class FRed, class FUpd>
+bool sanity_check(graph_csr_mipmapped<vT, eT, vIdxT> &h, graph_csr_mipmapped_device<vT, eT, vIdxT> &d,
+                  FInit fInit, FComp fComp, FRed fRed, FUpd fUpd) {
   return sanity_check(h.get_num_vertices(), h.V, h.R, h.C, h.E, d.V, fInit, fComp, fRed, fUpd);
 }
 

@@ -1,7 +1,7 @@
 // kites.cuh -- umbrella header of the kites:: API (farkhor/KiTES
 // kites/kites.cuh:4-14): #include "kites/kites.cuh" and link
-// libkites_b200.so.  Single-GPU only; the multi-device and "mipmapped"
-// graph classes of the reference are not provided.
+// libkites_b200.so.  Single-GPU only: the multi-device graph classes of
+// the reference are not provided.
 #ifndef KITES_B200_KITES_CUH_
 #define KITES_B200_KITES_CUH_
 
@@ -14,6 +14,8 @@
 #include "device/nv_gpu.cuh"
 #include "graph/graph_csr.h"
 #include "graph/graph_csr_device.cuh"
+#include "graph/graph_csr_mipmapped.hpp"
+#include "graph/graph_csr_mipmapped_device.cuh"
 #include "device/compute.cuh"
 #include "io/graph_output.cuh"
 #include "graph/sanity_check.cuh"

@@ -149,7 +149,7 @@ typedef struct kites_run_stats {
   uint64_t pull_kernel_bytes;       /* algorithmic bytes of those launches   */
   uint32_t n_recorded;
   uint8_t iter_strategy[KITES_MAX_RECORDED_ITERS];
-  float iter_ms[KITES_MAX_RECORDED_ITERS];
+  float iter_ms[KITES_MAX_RECORDED_ITERS];     /* time_kernels: each pull's time */
   uint64_t iter_active[KITES_MAX_RECORDED_ITERS];
   uint64_t iter_edges[KITES_MAX_RECORDED_ITERS];
   double pull_dense_ms;             /* time_kernels, PLAIN: the pulls of the

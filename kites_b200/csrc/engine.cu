@@ -526,6 +526,7 @@ int drive_loop(kites_graph *g, const kites_run_opts &o, loop_key key, Launch lau
         KITES_CUDA_TRY(cudaEventElapsedTime(&kms, eng->kev0, eng->kev1));
         st->pull_kernel_ms += kms;
         st->pull_kernel_launches += 1;
+        if (i < KITES_MAX_RECORDED_ITERS) st->iter_ms[i] = kms;
         g->pull_log.push_back({kms, prev_out_edges > g->dense_edges, hctr->last_active,
                                hctr->last_edges, hctr->total_updated});
       }
@@ -996,6 +997,7 @@ int run_auto(kites_graph *g, const kites_run_opts &o, kites_run_stats *st) {
         KITES_CUDA_TRY(cudaEventElapsedTime(&kms, eng->kev0, eng->kev1));
         st->pull_kernel_ms += kms;
         st->pull_kernel_launches += 1;
+        if (i < KITES_MAX_RECORDED_ITERS) st->iter_ms[i] = kms;
         g->pull_log.push_back({kms, prev_out_edges > g->dense_edges, hctr->last_active,
                                hctr->last_edges, hctr->total_updated});
       }

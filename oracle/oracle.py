@@ -8,6 +8,8 @@ Contents
   build_host_graph   restates graph_raw.h:57-190 + graph_csr.h:44-110 (the
                      host CSC, initial values, initial frontier bitmap,
                      128-padding and the vpg group out-adjacency) in numpy.
+  mipmap_of          the block frontier and block mipmap of
+                     graph_csr_mipmapped.hpp:40-78.
   sanity_check       kites/graph/sanity_check.cuh:22-47 (C, kites_oracle.c)
   process            kites/device/compute.cuh:29-137 + kernels_single_device.cuh
                      restated sequentially (C, kites_oracle.c)
@@ -236,6 +238,30 @@ def build_host_graph(first, second, weights=None, *, form_s_d=True, vpg=1,
     return HostGraph(V=Vp, R=R, C=C, E=E, vBitmap=_pack_bits(flags),
                      nbits=int(nbits), directed=directed, vertexPerGroup=vpg,
                      dir_R=dir_R, dir_C=dir_C, n_unpadded=n)
+
+
+def mipmap_of(hg: HostGraph, cr: int):
+    """The block structures kites::graph_csr_mipmapped adds to a directed
+    one-vertex-per-group host graph (graph_csr_mipmapped.hpp:40-78):
+    mipmapDim = ceil(n / cr) rounded up to a multiple of 32 (n the padded
+    vertex count); the block frontier, bit v // cr set for every vertex v
+    whose frontier bit is set; the mipmap, a mipmapDim x mipmapDim row-major
+    bit matrix with bit (s // cr) * mipmapDim + d // cr set for every edge
+    s -> d.  Returns (mipmapDim, frontier words, mipmap words)."""
+    assert hg.directed and hg.vertexPerGroup == 1 and cr > 0
+    n = hg.n_vertices
+    dim = -(-n // cr)
+    dim = -(-dim // 32) * 32
+    act = np.flatnonzero(unpack_bits(hg.vBitmap, hg.nbits)[:n])
+    blocks = np.zeros(dim, dtype=bool)
+    blocks[act // cr] = True
+    counts = np.diff(hg.dir_R.astype(np.int64))
+    src = np.repeat(np.arange(n, dtype=np.int64), counts)
+    bit = (src // cr) * dim + hg.dir_C.astype(np.int64) // cr
+    words = np.zeros(dim * dim // 32, dtype=np.uint32)
+    bit = np.unique(bit)
+    np.bitwise_or.at(words, bit >> 5, (np.uint32(1) << (bit & 31).astype(np.uint32)))
+    return dim, _pack_bits(blocks), words
 
 
 def example_weight_rule(src, dst):

@@ -10,6 +10,11 @@
 //       kites::sanity_check raw overload (kites/graph/sanity_check.cuh:13-59)
 //       over the built arrays.  Dumps every public member of the host graph
 //       plus the fixed point and the sweep count.
+//   mipmap <edgelist> <cr> <sd|ds> <source> <out>
+//       kites::graph_csr_mipmapped<unsigned,unsigned> with compression
+//       ratio cr from an edge-list file and the same pre-processing
+//       function (SSSP values); dumps V, R, C, E, the block frontier and the
+//       block mipmap (kites/graph/graph_csr_mipmapped.hpp:40-78).
 //   csc <in> <sssp_wrap|sssp_sat|bfs|cc> <out> [max_seconds]
 //       Reads a binary CSC and runs the reference's sanity_check loop on it
 //       with the four user functions of the chosen operator; dumps V and the
@@ -18,6 +23,7 @@
 // The functions below are this harness's own; the graph construction and
 // the fixed-point loop are the reference's code, included unmodified.
 #include "kites/graph/sanity_check.cuh"
+#include "kites/graph/graph_csr_mipmapped.hpp"
 
 #include <chrono>
 #include <cstdint>
@@ -131,6 +137,34 @@ int run_build(int argc, char **argv) {
   return 0;
 }
 
+int run_mipmap(int argc, char **argv) {
+  if (argc < 7) return 2;
+  const char *path = argv[2];
+  const unsigned cr = static_cast<unsigned>(atoi(argv[3]));
+  const bool sd = std::string(argv[4]) == "sd";
+  g_source = static_cast<unsigned>(strtoul(argv[5], nullptr, 10));
+  g_label_init = false;
+  const char *out = argv[6];
+  using vT = unsigned;
+  using eT = unsigned;
+  kites::graph_csr_mipmapped<vT, eT> g(
+      path, harness_preprocess<vT, eT>, cr,
+      sd ? kites::input_graph_form::edge_list_s_d : kites::input_graph_form::edge_list_d_s);
+  FILE *f = fopen(out, "wb");
+  if (!f) { perror(out); exit(3); }
+  uint64_t hdr[6] = {g.get_num_vertices(), g.get_num_edges(), g.compressionRatio,
+                     g.mipmapDim, g.vBitmap.size(), g.mipmap.size()};
+  put(f, hdr, 6);
+  put(f, g.V.get_ptr(), g.V.size());
+  put(f, g.R.get_ptr(), g.R.size());
+  put(f, g.C.get_ptr(), g.C.size());
+  put(f, g.E.get_ptr(), g.E.size());
+  put(f, g.vBitmap.get_ptr(), g.vBitmap.size());
+  put(f, g.mipmap.get_ptr(), g.mipmap.size());
+  fclose(f);
+  return 0;
+}
+
 int run_csc(int argc, char **argv) {
   if (argc < 5) return 2;
   std::string op = argv[3];
@@ -192,6 +226,7 @@ int main(int argc, char **argv) {
   try {
     if (argc >= 2 && std::string(argv[1]) == "build") return run_build(argc, argv);
     if (argc >= 2 && std::string(argv[1]) == "csc") return run_csc(argc, argv);
+    if (argc >= 2 && std::string(argv[1]) == "mipmap") return run_mipmap(argc, argv);
   } catch (const std::exception &e) {
     fprintf(stderr, "%s\n", e.what());
     return 4;

@@ -30,6 +30,7 @@ from oracle import oracle as O  # noqa: E402
 HARNESS = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
 OUT = os.path.join(ROOT, "tests", "golden", "golden.npz")
 
+MIPMAP_CRS = (1, 3, 32, 100)
 CFG1 = dict(scale=13, n_vertices=7115, n_edges=103689, a=0.57, b=0.19, c=0.19,
             seed=1, w_lo=1, w_hi=63)
 
@@ -71,6 +72,19 @@ def run_build(edge_file, vpg, source, init="sssp", directed=True, inf=None):
               if "performed" in line]
     d["sweeps"] = sweeps[0] if sweeps else -1
     return d
+
+
+def run_mipmap(edge_file, cr, source):
+    """The reference's graph_csr_mipmapped (SSSP values from `source`):
+    (mipmapDim, sha256 of V, R, C, E, block frontier words, mipmap words)."""
+    with tempfile.TemporaryDirectory() as td:
+        out = os.path.join(td, "dump.bin")
+        subprocess.run([HARNESS, "mipmap", edge_file, str(cr), "sd", str(source), out],
+                       check=True, capture_output=True)
+        with open(out, "rb") as f:
+            n, m, _, dim, nb, nm = (int(x) for x in np.frombuffer(f.read(48), np.uint64))
+            arrays = [np.frombuffer(f.read(4 * k), np.uint32) for k in (n, n + 1, m, m, nb, nm)]
+    return dim, sha(*arrays)
 
 
 def run_csc(R, C, E, V, op):
@@ -117,6 +131,13 @@ def main(argv=None):
             g["wiki_sssp"] = d["Vfix"]
             meta["wiki"]["sweeps"] = d["sweeps"]
             meta["wiki"]["n"] = d["n"]
+    # Mipmapped construction (graph_csr_mipmapped.hpp:40-78), block sizes
+    # 1, 3, 32 and 100.
+    meta["wiki"]["mipmap_dim"] = {}
+    for cr in MIPMAP_CRS:
+        dim, h = run_mipmap(wiki, cr, 30)
+        g[f"wiki_mipmap_cr{cr}"] = np.frombuffer(bytes.fromhex(h), np.uint8)
+        meta["wiki"]["mipmap_dim"][str(cr)] = dim
     # Undirected (incomplete edge list) construction: the reference copies no
     # frontier bits (graph_csr.h:100-101), so process() leaves V untouched.
     d = run_build(wiki, 1, 30, directed=False)
@@ -137,6 +158,11 @@ def main(argv=None):
             dv = run_build(ef, vpg, 0)
             g[f"cfg1_struct_vpg{vpg}"] = np.frombuffer(bytes.fromhex(struct_hash(dv)),
                                                        np.uint8)
+        meta["cfg1_mipmap_dim"] = {}
+        for cr in MIPMAP_CRS:
+            dim, h = run_mipmap(ef, cr, 0)
+            g[f"cfg1_mipmap_cr{cr}"] = np.frombuffer(bytes.fromhex(h), np.uint8)
+            meta["cfg1_mipmap_dim"][str(cr)] = dim
     hg = O.build_host_graph(s, t, w, init="source", source=0, inf=O.INF32)
     V0 = np.full(hg.n_vertices, O.INF32, np.uint32)
     V0[0] = 0

@@ -83,3 +83,45 @@ def test_example_runs_on_gpu(example_binary, cfg1_edges, tmp_path, vpg, builtin,
                             inf=EX_INF, weight_rule=None if weighted else example_weights)
     want, _ = O.process(hg, op=O.OP_SSSP_WRAP)
     np.testing.assert_array_equal(got, want)
+
+
+def test_mipmapped_example_compiles():
+    with tempfile.TemporaryDirectory() as td:
+        nvcc(os.path.join(ROOT, "examples", "sssp_mipmapped.cu"), os.path.join(td, "x"))
+
+
+@pytest.fixture(scope="module")
+def mipmapped_binary(tmp_path_factory):
+    d = tmp_path_factory.mktemp("mip")
+    exe = str(d / "sssp_mipmapped")
+    nvcc(os.path.join(ROOT, "examples", "sssp_mipmapped.cu"), exe)
+    return exe
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("cr", [1, 3, 32, 100])
+def test_mipmapped_runs_on_gpu(mipmapped_binary, cfg1_edges, tmp_path, cr):
+    """kites::graph_csr_mipmapped through make_graph_csr_for_device and the
+    coarse-activation process: the host block frontier and mipmap equal the
+    oracle's restatement of the reference's class, and the device distances
+    equal the oracle's fixed point (the same as over graph_csr: coarse
+    activation only adds work for a min-plus program)."""
+    s, d, w = cfg1_edges
+    ef = tmp_path / "edges.txt"
+    with open(ef, "w") as f:
+        for a, b, c in zip(s.tolist(), d.tolist(), w.tolist()):
+            f.write(f"{a}\t{b}\t{c}\n")
+    src = 17
+    pre = str(tmp_path / "out")
+    r = subprocess.run([mipmapped_binary, str(ef), str(src), str(cr), pre],
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "SANITY CHECK: PASSED" in r.stdout
+    hg = O.build_host_graph(s, d, w, init="source", source=src, inf=EX_INF)
+    dim, bits, mip = O.mipmap_of(hg, cr)
+    assert f"mipmapDim {dim}" in r.stdout
+    np.testing.assert_array_equal(np.fromfile(pre + ".bits", np.uint32), bits)
+    np.testing.assert_array_equal(np.fromfile(pre + ".mip", np.uint32), mip)
+    got = np.loadtxt(pre + ".dist", dtype=np.uint64).astype(np.uint32)
+    want, _ = O.process(hg, op=O.OP_SSSP_WRAP)
+    np.testing.assert_array_equal(got, want)

@@ -53,6 +53,35 @@ def test_builder_matches_reference_wiki(golden, has_reference, vpg):
     assert struct_hash(hg) == bytes(golden[f"wiki_struct_vpg{vpg}"])
 
 
+def mipmap_hash(hg, cr):
+    dim, bits, mip = O.mipmap_of(hg, cr)
+    return dim, edges_hash(hg.V, hg.R.astype(np.uint32), hg.C, hg.E, bits, mip)
+
+
+@pytest.mark.parametrize("cr", [1, 3, 32, 100])
+def test_mipmap_matches_reference_cfg1(golden, cfg1_edges, cr):
+    """kites::graph_csr_mipmapped's block frontier and mipmap, from the
+    reference's own class (graph_csr_mipmapped.hpp:40-78)."""
+    s, d, w = cfg1_edges
+    hg = O.build_host_graph(s, d, w, init="source", source=0, inf=EX_INF)
+    dim, h = mipmap_hash(hg, cr)
+    assert dim == golden["meta"]["cfg1_mipmap_dim"][str(cr)]
+    assert h == bytes(golden[f"cfg1_mipmap_cr{cr}"])
+
+
+@pytest.mark.parametrize("cr", [1, 3, 32, 100])
+def test_mipmap_matches_reference_wiki(golden, has_reference, cr):
+    if not has_reference:
+        pytest.skip("reference example file not present")
+    from conftest import WIKI
+    a, b, w = O.read_edge_list(WIKI)
+    hg = O.build_host_graph(a, b, w, init="source", source=30, inf=EX_INF,
+                            weight_rule=O.example_weight_rule)
+    dim, h = mipmap_hash(hg, cr)
+    assert dim == golden["meta"]["wiki"]["mipmap_dim"][str(cr)]
+    assert h == bytes(golden[f"wiki_mipmap_cr{cr}"])
+
+
 def test_wiki_fixed_point_and_process(golden, has_reference):
     if not has_reference:
         pytest.skip("reference example file not present")
