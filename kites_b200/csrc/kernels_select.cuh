@@ -84,7 +84,8 @@ __global__ void __launch_bounds__(256) k_select(select_args<OffT> a) {
   const uint32_t lane = lane_id(), wid = threadIdx.x >> 5;
   // A warp reads 32 changed-set words at once (one coalesced load, so an
   // empty stretch costs one load per 32 words); for each non-empty word a
-  // lane takes one bit, so the degree loads of its vertices are coalesced.
+  // lane takes one bit, so the degree loads of its vertices are coalesced,
+  // and the loads of up to 8 non-empty words are in flight together.
   const uint64_t nwarps = (uint64_t)gridDim.x * (blockDim.x >> 5);
   for (uint64_t base = (((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32;
        base < a.nwords; base += nwarps * 32) {
@@ -92,16 +93,27 @@ __global__ void __launch_bounds__(256) k_select(select_args<OffT> a) {
     const uint32_t word = wl < a.nwords ? a.U[wl] : 0u;
     uint32_t nz = __ballot_sync(kFull, word != 0u);
     while (nz) {
-      const uint32_t i = __ffs(nz) - 1;
-      nz &= nz - 1;
-      const uint32_t bits = __shfl_sync(kFull, word, i);
-      if (!((bits >> lane) & 1u)) continue;
-      const uint64_t v = (base + i) * 32 + lane;
-      const uint32_t od = a.out_deg[v];
-      ++c;
-      os += od;
-      om = max(om, od);
-      is += (unsigned long long)(a.R[v + 1] - a.R[v]);
+      constexpr int kRound = 8;
+      uint32_t od[kRound];
+      OffT r0[kRound], r1[kRound];
+#pragma unroll
+      for (int q = 0; q < kRound; ++q) {
+        const uint32_t i = nz ? (uint32_t)(__ffs(nz) - 1) : 32u;
+        nz &= nz - 1;
+        const uint32_t bits = __shfl_sync(kFull, word, i & 31u);
+        const bool on = i < 32u && ((bits >> lane) & 1u);
+        const uint64_t v = (base + (i & 31u)) * 32 + lane;
+        od[q] = on ? a.out_deg[v] : 0u;
+        r0[q] = on ? a.R[v] : (OffT)0;
+        r1[q] = on ? a.R[v + 1] : (OffT)0;
+        c += on ? 1u : 0u;
+      }
+#pragma unroll
+      for (int q = 0; q < kRound; ++q) {
+        os += od[q];
+        om = max(om, od[q]);
+        is += (unsigned long long)(r1[q] - r0[q]);
+      }
     }
   }
   c = __reduce_add_sync(kFull, (uint32_t)c);
