@@ -355,14 +355,16 @@ void launch_sweep(kites_graph *g, const uint32_t *rd, const uint32_t *U, uint32_
 template <typename OffT>
 void launch_expand(kites_graph *g, const void *aR, const uint32_t *aC, const uint32_t *chunks,
                    uint64_t nchunks, bool dense_pull, uint64_t rows, uint64_t edges,
-                   const uint32_t *chg, uint32_t *wr, uint32_t gate_cur, uint64_t *launches) {
+                   const uint32_t *chg, uint32_t *wr, uint32_t gate_cur, uint64_t *launches,
+                   bool dense_by_next_pull = false) {
   cudaStream_t s = g->eng->stream;
   const bool sweep = dense_pull && g->rowid != nullptr;
   chunk_geom<OffT> ga{(const OffT *)aR, aC, chunks, nchunks, rows, rows + edges, g->chunk_items};
   expand_args<OffT> ea{ga, chg, wr, g->ctr, sweep ? 1u : 0u, gate_cur, g->dense_rows};
   k_expand_chunked<OffT><<<g->expand_grid, kBlock, 0, s>>>(ea);
   ++*launches;
-  if (sweep) {
+  // A dense changed set is left to the next iteration's k_sweep_changed.
+  if (sweep && !dense_by_next_pull) {
     sweep_args<OffT> sa{(const OffT *)g->R, g->C, nullptr, g->rowid, nullptr, g->m, g->n,
                         nullptr, chg, wr, g->ctr, 2u, gate_cur, g->dense_rows};
     k_activate_sweep<OffT><<<g->sweep_grid, kSweepThreads, 0, s>>>(sa);
@@ -371,6 +373,11 @@ void launch_expand(kites_graph *g, const void *aR, const uint32_t *aC, const uin
 }
 
 // One iteration of the plain strategy: pull, activation, clear, check.
+// Bitmaps of parity p: frontier[p] is read (F_t), changed[p] written (U_t),
+// activation writes frontier[p^1].  With edge sweeps (vpg == 1) a dense
+// changed set is not expanded: the next iteration's k_sweep_changed finds
+// its rows from U_t itself, so U_t (changed[p]) is kept one iteration
+// longer and cleared at the end of the next one.
 template <int OP, typename OffT>
 int launch_iteration(kites_graph *g, int parity, cudaGraphConditionalHandle h,
                      int has_handle, uint64_t *launches, bool time_pull) {
@@ -378,26 +385,37 @@ int launch_iteration(kites_graph *g, int parity, cudaGraphConditionalHandle h,
   if (time_pull) KITES_CUDA_TRY(cudaEventRecord(g->eng->kev0, s));
   chunk_geom<OffT> gin{(const OffT *)g->R, g->C, g->chunk_in, g->nchunks_in,
                        g->n, g->n + g->m, g->chunk_items};
-  // Sparse frontiers: per-row chunked pull; dense ones (activation edges of
-  // the previous iteration above dense_edges): the staged sweep.  Both are
-  // launched, the gate lets exactly one do the work.
+  // Three pulls are launched and the gates let exactly one work: after a
+  // dense changed set, k_sweep_changed; else on a sparse frontier the
+  // per-row chunked pull, on a dense one (activation edges of the previous
+  // iteration above dense_edges) the edge sweep.
   const bool sweep = g->rowid != nullptr;
   pull_args<OffT> pa{gin, (const uint32_t *)g->E, (uint32_t *)g->V,
                      g->frontier[parity], g->changed[parity], g->shift, g->ctr, nullptr,
-                     sweep ? 1u : 0u, 0u, g->dense_edges};
+                     sweep ? 1u : 0u, 0u, g->dense_edges, sweep ? g->dense_rows : 0ull};
   k_pull_chunked<OP, OffT><<<g->pull_grid, kBlock, 0, s>>>(pa);
   if (sweep) {
     launch_sweep<OP, OffT, kRowFilter>(g, g->frontier[parity], nullptr, g->changed[parity],
                                        2u, 0u);
-    ++*launches;
+    sweep_args<OffT> fa{(const OffT *)g->R, g->C, (const uint32_t *)g->E, g->rowid,
+                        (uint32_t *)g->V, g->m, g->n, nullptr, g->changed[parity ^ 1],
+                        g->changed[parity], g->ctr, 0u, 0u, g->dense_rows,
+                        g->frontier[parity]};
+    k_sweep_changed<OP, OffT><<<g->sweep_grid, kSweepThreads, 0, s>>>(fa);
+    *launches += 2;
   }
   if (time_pull) KITES_CUDA_TRY(cudaEventRecord(g->eng->kev1, s));
   launch_expand<OffT>(g, g->dirR, g->dirC, g->chunk_dir, g->nchunks_dir, g->vpg == 1,
                       g->n_dir_rows, g->n_dir_edges, g->changed[parity],
-                      g->frontier[parity ^ 1], 1u, launches);
-  // Clear the read frontier and the changed bitmap (adjacent words).
-  k_clear_words<<<grid_for(2 * g->nwords, 256, 4096), 256, 0, s>>>(g->frontier[parity],
-                                                                    2 * g->nwords);
+                      g->frontier[parity ^ 1], 1u, launches, sweep);
+  // Clear the read frontier and, with sweeps, the previous changed set;
+  // without them this iteration's (adjacent words).
+  if (sweep)
+    k_clear_two<<<grid_for(g->nwords, 256, 4096), 256, 0, s>>>(g->frontier[parity],
+                                                                g->changed[parity ^ 1], g->nwords);
+  else
+    k_clear_words<<<grid_for(2 * g->nwords, 256, 4096), 256, 0, s>>>(g->frontier[parity],
+                                                                      2 * g->nwords);
   iter_record rec{g->rec_active, g->rec_edges, KITES_MAX_RECORDED_ITERS};
   k_loop_check<<<1, 1, 0, s>>>(g->ctr, rec, h, has_handle);
   KITES_CUDA_TRY(cudaGetLastError());
@@ -514,8 +532,9 @@ int drive_loop(kites_graph *g, const kites_run_opts &o, loop_key key, Launch lau
   } else {
     KITES_CUDA_TRY(cudaEventRecord(eng->ev0, s));
     g->pull_log.clear();
-    // The sweeps' gate reads the previous iteration's activation edges.
-    unsigned long long prev_out_edges = 0;
+    // The sweeps' gates read the previous iteration's activation edges and
+    // changed rows.
+    unsigned long long prev_out_edges = 0, prev_changed = 0;
     for (uint64_t i = 0;; ++i) {
       KITES_TRY(launch((int)(i & 1), 0, 0, launches, o.time_kernels != 0));
       KITES_CUDA_TRY(cudaMemcpyAsync(hctr, g->ctr, sizeof(run_counters),
@@ -527,10 +546,13 @@ int drive_loop(kites_graph *g, const kites_run_opts &o, loop_key key, Launch lau
         st->pull_kernel_ms += kms;
         st->pull_kernel_launches += 1;
         if (i < KITES_MAX_RECORDED_ITERS) st->iter_ms[i] = kms;
-        g->pull_log.push_back({kms, prev_out_edges > g->dense_edges, hctr->last_active,
-                               hctr->last_edges, hctr->total_updated});
+        const bool dense = prev_out_edges > g->dense_edges ||
+                           (g->rowid && prev_changed > g->dense_rows);
+        g->pull_log.push_back({kms, dense, hctr->last_active, hctr->last_edges,
+                               hctr->total_updated});
       }
       prev_out_edges = hctr->last_out_edges;
+      prev_changed = hctr->last_changed;
       if (hctr->done) break;
     }
   }
@@ -566,6 +588,10 @@ int run_plain(kites_graph *g, const kites_run_opts &o, kites_run_stats *st) {
   auto launch = [g](int parity, cudaGraphConditionalHandle h, int hh, uint64_t *l, bool tp) {
     return launch_iteration<OP, OffT>(g, parity, h, hh, l, tp);
   };
+  // Both changed sets start empty (the first iteration reads changed[1] as
+  // the previous one's).
+  KITES_CUDA_TRY(cudaMemsetAsync(g->changed[0], 0, g->nwords * 4, g->eng->stream));
+  KITES_CUDA_TRY(cudaMemsetAsync(g->changed[1], 0, g->nwords * 4, g->eng->stream));
   KITES_TRY(drive_loop(g, o, loop_key{OP, KITES_STRATEGY_PLAIN}, launch, &c, &ms, &launches, st));
   if (st) {
     st->iterations = c.iterations;
@@ -979,8 +1005,9 @@ int run_auto(kites_graph *g, const kites_run_opts &o, kites_run_stats *st) {
   } else {
     KITES_CUDA_TRY(cudaEventRecord(eng->ev0, s));
     g->pull_log.clear();
-    // The sweeps' gate reads the previous iteration's activation edges.
-    unsigned long long prev_out_edges = 0;
+    // The sweeps' gates read the previous iteration's activation edges and
+    // changed rows.
+    unsigned long long prev_out_edges = 0, prev_changed = 0;
     for (uint64_t i = 0;; ++i) {
       const int parity = (int)(i & 1);
       KITES_TRY(launch_select<OffT>(g, f.U[parity], o.selector_margin, nullptr, 0, 0, 0,
@@ -998,10 +1025,13 @@ int run_auto(kites_graph *g, const kites_run_opts &o, kites_run_stats *st) {
         st->pull_kernel_ms += kms;
         st->pull_kernel_launches += 1;
         if (i < KITES_MAX_RECORDED_ITERS) st->iter_ms[i] = kms;
-        g->pull_log.push_back({kms, prev_out_edges > g->dense_edges, hctr->last_active,
-                               hctr->last_edges, hctr->total_updated});
+        const bool dense = prev_out_edges > g->dense_edges ||
+                           (g->rowid && prev_changed > g->dense_rows);
+        g->pull_log.push_back({kms, dense, hctr->last_active, hctr->last_edges,
+                               hctr->total_updated});
       }
       prev_out_edges = hctr->last_out_edges;
+      prev_changed = hctr->last_changed;
       if (hctr->done) break;
     }
   }

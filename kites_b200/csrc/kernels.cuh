@@ -156,6 +156,10 @@ struct pull_args {
   // iteration's when gate_cur, else the previous one's) above dense_edges.
   uint32_t gate, gate_cur;
   unsigned long long dense_edges;
+  // PLAIN with the fused dense step: when the previous iteration's changed
+  // rows exceed fused_rows (0 = off), k_sweep_changed pulls from them and
+  // this kernel has nothing to do.
+  unsigned long long fused_rows;
 };
 
 __device__ __forceinline__ bool frontier_dense(const run_counters *c, uint32_t cur,
@@ -281,6 +285,7 @@ template <int OP, typename OffT>
 __global__ void __launch_bounds__(kBlock) k_pull_chunked(pull_args<OffT> a) {
   if (a.ctr->done) return;
   if (a.gate == 1 && frontier_dense(a.ctr, a.gate_cur, a.dense_edges)) return;
+  if (a.fused_rows && a.ctr->last_changed > a.fused_rows) return;
   pull_chunks<OP, OffT, false>(a);
 }
 

@@ -3,12 +3,15 @@
 //
 // One in-edge read serves all K sources: a warp walks the active vertices
 // of an edge-balanced chunk one at a time; it loads 32 (C, E) pairs with
-// one coalesced load, then for each edge the lanes -- one per source slice
-// -- gather the source vertex's whole K-wide row (64 B .. 1 KB, contiguous)
-// and fold it into their running minima.  K = LPE x VPL with LPE lanes per
-// edge and VPL values per lane (vector loads); for K = 16 two edges are in
-// flight per warp step.  A vertex whose in-edges span several chunks merges
-// its partial rows with atomicMin, like the single-source kernel.
+// one coalesced load, then for each edge a group of lanes gathers the
+// source vertex's whole K-wide row (64 B .. 1 KB, contiguous) and folds it
+// into its running minima.  Each lane moves 8 values (32 bytes) of a row
+// with one 256-bit load (ld.global.v8.b32, new with sm_100), so a row takes
+// K/8 lanes and a warp step covers 32/(K/8) edges; four steps' rows are
+// loaded before any is folded (16 source rows in flight per warp for
+// K = 64).  The lane groups' minima of a row meet over shuffles.  A vertex
+// whose in-edges span several chunks merges its partial rows with
+// atomicMin, like the single-source kernel.
 #pragma once
 #include "kernels.cuh"
 
@@ -16,9 +19,9 @@ namespace kites_internal {
 
 template <int K>
 struct batch_shape {
-  static constexpr int LPE = K >= 32 ? 32 : K;  // lanes per edge
-  static constexpr int VPL = K / LPE;           // values per lane
-  static constexpr int EPW = 32 / LPE;          // edges per warp step
+  static constexpr int VPL = 8;          // values per lane: one 32-byte access
+  static constexpr int LPE = K / VPL;    // lanes per edge (a K-wide row)
+  static constexpr int EPW = 32 / LPE;   // edges per warp step
   static_assert(K == 16 || K == 32 || K == 64 || K == 128 || K == 256, "K");
 };
 
@@ -52,9 +55,26 @@ __device__ __forceinline__ void store_row(uint32_t *p, const uint32_t (&x)[VPL])
   }
 }
 
-// Source rows each lane group keeps in flight: 8 x K/LPE values per lane.
+// One 32-byte access per lane (the address is 32-byte aligned: rows start at
+// multiples of K >= 16 values and each lane's slice at a multiple of 8).
+__device__ __forceinline__ void load_row8(const uint32_t *p, uint32_t (&x)[8]) {
+  asm volatile("ld.global.v8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+               : "=r"(x[0]), "=r"(x[1]), "=r"(x[2]), "=r"(x[3]), "=r"(x[4]), "=r"(x[5]),
+                 "=r"(x[6]), "=r"(x[7])
+               : "l"(p));
+}
+__device__ __forceinline__ void store_row8(uint32_t *p, const uint32_t (&x)[8]) {
+  asm volatile("st.global.v8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};"
+               :: "l"(p), "r"(x[0]), "r"(x[1]), "r"(x[2]), "r"(x[3]), "r"(x[4]), "r"(x[5]),
+                  "r"(x[6]), "r"(x[7]) : "memory");
+}
+
+// Source rows each lane group keeps in flight.  Four, at 64 registers and
+// four CTAs per SM, spill 152 bytes per thread and still beat two rows
+// without spills by 8 % (R-MAT scale 24, K = 64); six and eight spill more
+// and are slower.
 template <int K>
-constexpr int rows_in_flight() { return K >= 128 ? 4 : 8; }
+constexpr int rows_in_flight() { return 4; }
 
 template <typename OffT>
 struct pull_batch_args {
@@ -123,7 +143,7 @@ __global__ void __launch_bounds__(kBlock, K >= 256 ? 2 : 4)
               const uint32_t u = __shfl_sync(kFull, cC, j & 31u);
               wq[r] = __shfl_sync(kFull, cE, j & 31u);
               if (j < ntile) {
-                load_row<S::VPL>(a.D + (uint64_t)u * K + kl * S::VPL, row[r]);
+                load_row8(a.D + (uint64_t)u * K + kl * S::VPL, row[r]);
               } else {
 #pragma unroll
                 for (int q = 0; q < S::VPL; ++q) row[r][q] = kInf;
@@ -137,22 +157,23 @@ __global__ void __launch_bounds__(kBlock, K >= 256 ? 2 : 4)
             }
           }
         }
-        if (S::EPW == 2) {
 #pragma unroll
-          for (int q = 0; q < S::VPL; ++q) acc[q] = min(acc[q], __shfl_xor_sync(kFull, acc[q], 16));
+        for (int d = S::LPE; d < 32; d <<= 1) {
+#pragma unroll
+          for (int q = 0; q < S::VPL; ++q) acc[q] = min(acc[q], __shfl_xor_sync(kFull, acc[q], d));
         }
         bool lane_upd = false;
         if (sub == 0) {
           uint32_t *dv = a.D + v * K + kl * S::VPL;
           uint32_t cur[S::VPL];
-          load_row<S::VPL>(dv, cur);
+          load_row8(dv, cur);
           if (whole) {
             bool any = false;
 #pragma unroll
             for (int q = 0; q < S::VPL; ++q) {
               if (acc[q] < cur[q]) { cur[q] = acc[q]; any = true; }
             }
-            if (any) { store_row<S::VPL>(dv, cur); lane_upd = true; }
+            if (any) { store_row8(dv, cur); lane_upd = true; }
           } else {
 #pragma unroll
             for (int q = 0; q < S::VPL; ++q)

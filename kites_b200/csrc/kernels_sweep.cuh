@@ -52,6 +52,7 @@ struct sweep_args {
   // Density gate (see pull_args / expand_args): 2 = run only when dense.
   uint32_t gate, gate_cur;
   unsigned long long dense_edges;
+  uint32_t *act;             // k_sweep_changed: the rows found active
 };
 
 constexpr uint32_t kNoRow = 0xFFFFFFFFu;
@@ -284,6 +285,130 @@ __global__ void __launch_bounds__(kSweepThreads, kSweepMinBlocks) k_sweep(sweep_
   if (lane == 0) {
     if (n_act) atomicAdd(&a.ctr->active, (unsigned long long)n_act);
     if (n_edges) atomicAdd(&a.ctr->edges, (unsigned long long)n_edges);
+    if (n_chg) atomicAdd(&a.ctr->changed, (unsigned long long)n_chg);
+  }
+}
+
+// PLAIN over a dense changed set without a materialised frontier (the
+// activation of the previous iteration and this pull in one pass).  Row v
+// is active iff one of its in-edges comes from a vertex of U, the previous
+// iteration's changed set -- exactly the rows the activation would have
+// set -- and only those in-edges are folded: an in-edge from a source that
+// did not change was folded when that source last changed (the change
+// activated v for the iteration after it), so it cannot lower v, and the
+// fixed point and the per-iteration work are the plain strategy's.  The V
+// gather of an edge is issued only when its source changed.  Counts as the
+// plain pull: a row's activity bit goes into `act` with atomicOr, and the
+// thread that sets it counts the row and its in-degree.
+// Gate: run only when U has more than dense_edges rows (here the changed-row
+// threshold), read from the counters of the previous iteration.
+template <int OP, typename OffT>
+__global__ void __launch_bounds__(kSweepThreads, kSweepMinBlocks)
+    k_sweep_changed(sweep_args<OffT> a) {
+  if (a.ctr->done) return;
+  if (!changed_dense(a.ctr, a.gate_cur, a.dense_edges)) return;
+  constexpr bool kW = op_reads_weights<OP>();
+  const uint32_t lane = lane_id();
+  unsigned long long n_act = 0, n_edges = 0;
+  uint32_t n_chg = 0;
+  bool any_upd = false;
+  auto mark = [&](uint32_t r) {
+    const uint32_t bit = 1u << (r & 31u);
+    if (bit & ~atomicOr(a.act + (r >> 5), bit)) {
+      ++n_act;
+      n_edges += (unsigned long long)(a.R[r + 1] - a.R[r]);
+    }
+  };
+  auto lower = [&](uint32_t r, uint32_t q) {
+    if (q < atomicMin(a.V + r, q)) {
+      any_upd = true;
+      n_chg += __popc((1u << (r & 31u)) & ~atomicOr(a.chg + (r >> 5), 1u << (r & 31u)));
+    }
+  };
+  const uint64_t warps = (uint64_t)gridDim.x * (kSweepThreads / 32);
+  for (uint64_t win = ((uint64_t)blockIdx.x * kSweepThreads + threadIdx.x) >> 5;
+       win * kWindowEdges < a.m; win += warps) {
+    const uint64_t e0 = win * kWindowEdges + (uint64_t)lane * kEdgesPerThread;
+    uint32_t row[kEdgesPerThread], src[kEdgesPerThread], wt[kEdgesPerThread];
+    load_edges8(a.rowid, a.C, e0, a.m, row, src);
+    if (kW) load_vals8(a.E, e0, a.m, wt);
+    if (__all_sync(kFull, e0 + kEdgesPerThread <= a.m)) {
+      uint32_t mx = 0;
+#pragma unroll
+      for (int k = 0; k < kEdgesPerThread; ++k) mx = max(mx, max(row[k], src[k]));
+      const bool bad = mx >= a.n_rows || row[0] > row[kEdgesPerThread - 1];
+      if (bad) a.ctr->error = 1u;  // never index with an id out of range
+      uint32_t hit[kEdgesPerThread], cand[kEdgesPerThread];
+#pragma unroll
+      for (int k = 0; k < kEdgesPerThread; ++k) {
+        const uint32_t uw = bad ? 0u : a.U[src[k] >> 5];
+        hit[k] = (uw >> (src[k] & 31u)) & 1u;
+      }
+#pragma unroll
+      for (int k = 0; k < kEdgesPerThread; ++k)
+        cand[k] = hit[k] ? nbr_comp<OP>(a.V[src[k]], wt[k]) : kInf;
+      const uint32_t r0 = bad ? kNoRow : row[0];
+      const uint32_t r7 = bad ? kNoRow : row[kEdgesPerThread - 1];
+      const uint32_t old_first = bad ? 0u : a.V[r0];
+      const uint32_t old_last = bad ? 0u : a.V[r7];
+      // Runs of equal row: p the running minimum, h whether a source changed.
+      uint32_t p = cand[0], fp = kInf, h = hit[0], fh = 0;
+#pragma unroll
+      for (int k = 1; k < kEdgesPerThread; ++k) {
+        const bool same = row[k] == row[k - 1];
+        if (!same && !bad) {
+          if (row[k - 1] == r0) {
+            fp = p;  // the first run ends
+            fh = h;
+          } else if (h) {  // a row wholly inside this thread
+            mark(row[k - 1]);
+            if (p != kInf) lower(row[k - 1], p);
+          }
+        }
+        p = same ? min(p, cand[k]) : cand[k];
+        h = same ? (h | hit[k]) : hit[k];
+      }
+      uint32_t lr = kNoRow, lp = kInf, lh = 0;
+      if (r7 == r0) { fp = p; fh = h; }
+      else { lr = r7; lp = p; lh = h; }
+#pragma unroll
+      for (int side = 0; side < 2; ++side) {
+        const uint32_t r = side ? lr : r0;
+        bool head;
+        const uint32_t rm = run_mask(r, &head);
+        const uint32_t q = __reduce_min_sync(rm, side ? lp : fp);
+        const uint32_t qh = __reduce_or_sync(rm, side ? lh : fh);
+        if (head && r != kNoRow && qh) {
+          mark(r);
+          if (q < (side ? old_last : old_first)) lower(r, q);
+        }
+      }
+      continue;
+    }
+    // The last window: edge by edge (at most 256 edges per launch).
+#pragma unroll
+    for (int k = 0; k < kEdgesPerThread; ++k) {
+      if (row[k] == kNoRow) continue;
+      if (src[k] >= a.n_rows || row[k] >= a.n_rows) {
+        a.ctr->error = 1u;  // never index with an id out of range
+        continue;
+      }
+      if (!((a.U[src[k] >> 5] >> (src[k] & 31u)) & 1u)) continue;
+      mark(row[k]);
+      const uint32_t c = nbr_comp<OP>(a.V[src[k]], wt[k]);
+      if (c < a.V[row[k]]) lower(row[k], c);
+    }
+  }
+  if (__any_sync(kFull, any_upd) && lane == 0) a.ctr->update_flag = 1u;
+  n_chg = __reduce_add_sync(kFull, n_chg);
+#pragma unroll
+  for (int d = 16; d; d >>= 1) {
+    n_act += __shfl_xor_sync(kFull, n_act, d);
+    n_edges += __shfl_xor_sync(kFull, n_edges, d);
+  }
+  if (lane == 0) {
+    if (n_act) atomicAdd(&a.ctr->active, n_act);
+    if (n_edges) atomicAdd(&a.ctr->edges, n_edges);
     if (n_chg) atomicAdd(&a.ctr->changed, (unsigned long long)n_chg);
   }
 }
