@@ -485,16 +485,16 @@ def run_ours(args):
                          if b_ach is not None else
                          {"bound": "hbm", "achieved": p_ach, "peak": peak, "unit": "GB/s",
                           "frac": p_ach / peak, "traffic": None,
-                          "kernel": "k_pull_chunked + k_sweep<SSSP> (plain pull)",
+                          "kernel": "k_pull_chunked + k_sweep + k_sweep_changed<SSSP> (plain pull)",
                           "launches": k_launch, "peak_source": src_note}),
             "roofline_plain": {"bound": "hbm", "achieved": p_ach, "peak": peak,
                                "unit": "GB/s", "frac": p_ach / peak,
-                               "kernel": "k_pull_chunked + k_sweep<SSSP> (plain pull phase)",
+                               "kernel": "k_pull_chunked + k_sweep + k_sweep_changed<SSSP> (plain pull phase)",
                                "launches": k_launch,
                                "peak_source": src_note},
             "roofline_plain_dense": ({"bound": "hbm", "achieved": d_ach, "peak": peak,
                                       "unit": "GB/s", "frac": d_ach / peak,
-                                      "kernel": "k_sweep<SSSP, row filter> (dense iterations)",
+                                      "kernel": "k_sweep<SSSP, row filter> + k_sweep_changed<SSSP> (dense iterations)",
                                       "launches": d_launch, "peak_source": src_note}
                                      if d_ach is not None else None),
             "cpu_baseline": cpu,

@@ -546,10 +546,9 @@ int drive_loop(kites_graph *g, const kites_run_opts &o, loop_key key, Launch lau
         st->pull_kernel_ms += kms;
         st->pull_kernel_launches += 1;
         if (i < KITES_MAX_RECORDED_ITERS) st->iter_ms[i] = kms;
-        const bool dense = prev_out_edges > g->dense_edges ||
-                           (g->rowid && prev_changed > g->dense_rows);
-        g->pull_log.push_back({kms, dense, hctr->last_active, hctr->last_edges,
-                               hctr->total_updated});
+        const bool fused = g->rowid && prev_changed > g->dense_rows;
+        g->pull_log.push_back({kms, fused || prev_out_edges > g->dense_edges, fused,
+                               hctr->last_active, hctr->last_edges, hctr->total_updated});
       }
       prev_out_edges = hctr->last_out_edges;
       prev_changed = hctr->last_changed;
@@ -606,25 +605,27 @@ int run_plain(kites_graph *g, const kites_run_opts &o, kites_run_stats *st) {
                             (8ull + e_bytes) * c.total_edges + 12ull * c.total_updated +
                             8ull * c.total_out_edges;
     st->strategy_hist[KITES_STRATEGY_PLAIN] += c.iterations;
-    if (o.time_kernels)
-      // Pull kernel alone: frontier words, 12 B per active vertex (V[v],
-      // R[v], R[v+1]), (4 C + eT + 4 V[src]) per in-edge, 4 B per store.
-      st->pull_kernel_bytes = c.iterations * 4ull * ((g->nbits + 31) / 32) +
-                              12ull * c.total_active + (8ull + e_bytes) * c.total_edges +
-                              4ull * c.total_updated;
-    if (o.time_kernels && g->rowid) {
-      // The iterations whose pull ran as the dense sweep, alone: the same
-      // algorithmic bytes as above, per iteration.
+    if (o.time_kernels) {
+      // Pull kernels alone, per iteration: frontier words, 12 B per active
+      // vertex (V[v], R[v], R[v+1]), (4 C + eT + 4 V[src]) per in-edge, 4 B
+      // per store.  A fused iteration (k_sweep_changed) also does the
+      // activation of the previous changed set in pull form: every
+      // in-edge's source and its changed-set word (4 + 4 bytes for all m
+      // edges) in place of the frontier words.  `pull_dense_*`: the
+      // iterations whose pull ran as a dense sweep.
       const uint64_t fw = 4ull * ((g->nbits + 31) / 32);
       unsigned long long upd_before = 0;
       for (const auto &r : g->pull_log) {
+        const uint64_t b = 12ull * r.active + (8ull + e_bytes) * r.edges +
+                           4ull * (r.total_updated - upd_before) +
+                           (r.fused ? 8ull * g->m - 4ull * r.edges : fw);
+        upd_before = r.total_updated;
+        st->pull_kernel_bytes += b;
         if (r.dense) {
           st->pull_dense_ms += r.ms;
           st->pull_dense_launches += 1;
-          st->pull_dense_bytes += fw + 12ull * r.active + (8ull + e_bytes) * r.edges +
-                                  4ull * (r.total_updated - upd_before);
+          st->pull_dense_bytes += b;
         }
-        upd_before = r.total_updated;
       }
     }
     st->kernel_launches += launches;
@@ -1025,10 +1026,9 @@ int run_auto(kites_graph *g, const kites_run_opts &o, kites_run_stats *st) {
         st->pull_kernel_ms += kms;
         st->pull_kernel_launches += 1;
         if (i < KITES_MAX_RECORDED_ITERS) st->iter_ms[i] = kms;
-        const bool dense = prev_out_edges > g->dense_edges ||
-                           (g->rowid && prev_changed > g->dense_rows);
-        g->pull_log.push_back({kms, dense, hctr->last_active, hctr->last_edges,
-                               hctr->total_updated});
+        const bool fused = g->rowid && prev_changed > g->dense_rows;
+        g->pull_log.push_back({kms, fused || prev_out_edges > g->dense_edges, fused,
+                               hctr->last_active, hctr->last_edges, hctr->total_updated});
       }
       prev_out_edges = hctr->last_out_edges;
       prev_changed = hctr->last_changed;

@@ -115,6 +115,7 @@ struct kites_graph {
   struct pull_rec {
     float ms;
     bool dense;
+    bool fused;   // the pull also found its rows from the previous changed set
     unsigned long long active, edges, total_updated;
   };
   std::vector<pull_rec> pull_log;
