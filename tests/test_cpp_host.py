@@ -1,0 +1,64 @@
+"""The host-side construction of the kites:: C++ front-end, on the CPU.
+
+tests/cpp/host_graphs.cpp builds kites::graph_csr (vertex groups 1, 2, 4, 8)
+and kites::graph_csr_mipmapped (block sizes 1, 3, 32, 100) from the
+config-1 edge list with g++, linked against host-memory stand-ins for the
+four CUDA runtime calls the host buffers make (tests/cpp/host_runtime_stub.cpp),
+and every array must hash to the golden value the reference's own classes
+produced (tests/golden/make_golden.py)."""
+import hashlib
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+CPP = os.path.join(ROOT, "tests", "cpp")
+
+
+def sha(*arrays):
+    h = hashlib.sha256()
+    for a in arrays:
+        h.update(np.ascontiguousarray(a).tobytes())
+    return h.digest()
+
+
+@pytest.fixture(scope="module")
+def tool(tmp_path_factory):
+    exe = str(tmp_path_factory.mktemp("hg") / "host_graphs")
+    subprocess.run(["g++", "-std=c++17", "-O2", "-I", os.path.join(ROOT, "include"),
+                    "-I", "/usr/local/cuda/include", "-o", exe,
+                    os.path.join(CPP, "host_graphs.cpp"), os.path.join(CPP, "host_runtime_stub.cpp")],
+                   check=True, capture_output=True)
+    return exe
+
+
+@pytest.fixture(scope="module")
+def cfg1_file(cfg1_edges, tmp_path_factory):
+    s, d, w = cfg1_edges
+    path = tmp_path_factory.mktemp("cfg1") / "edges.txt"
+    with open(path, "w") as f:
+        for a, b, c in zip(s.tolist(), d.tolist(), w.tolist()):
+            f.write(f"{a}\t{b}\t{c}\n")
+    return str(path)
+
+
+def dump(tool, mode, edges, param, out):
+    subprocess.run([tool, mode, edges, str(param), "0", str(out)], check=True, capture_output=True)
+    with open(out, "rb") as f:
+        counts = [int(x) for x in np.frombuffer(f.read(56), np.uint64)]
+        return [np.frombuffer(f.read(4 * k), np.uint32) for k in counts[:6 if mode == "mip" else 7]], counts
+
+
+@pytest.mark.parametrize("vpg", [1, 2, 4, 8])
+def test_graph_csr_matches_reference(tool, cfg1_file, golden, tmp_path, vpg):
+    (V, R, C, E, bits, dR, dC), _ = dump(tool, "csr", cfg1_file, vpg, tmp_path / "d.bin")
+    assert sha(R, C, E, V, bits, dR, dC) == bytes(golden[f"cfg1_struct_vpg{vpg}"])
+
+
+@pytest.mark.parametrize("cr", [1, 3, 32, 100])
+def test_graph_csr_mipmapped_matches_reference(tool, cfg1_file, golden, tmp_path, cr):
+    (V, R, C, E, bits, mip), counts = dump(tool, "mip", cfg1_file, cr, tmp_path / "d.bin")
+    assert counts[6] == golden["meta"]["cfg1_mipmap_dim"][str(cr)]
+    assert sha(V, R, C, E, bits, mip) == bytes(golden[f"cfg1_mipmap_cr{cr}"])
