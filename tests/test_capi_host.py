@@ -53,6 +53,7 @@ int main(void) {
   P(kites_csc_view, on_device) P(kites_csc_view, frontier_nbits)
   P(kites_device_view, stream) P(kites_run_opts, time_kernels)
   P(kites_run_stats, pull_kernel_bytes) P(kites_run_stats, iter_edges)
+  P(kites_run_stats, pull_dense_bytes) P(kites_csc_view, offsets64)
   return 0;
 }
 """
@@ -73,6 +74,8 @@ int main(void) {
     assert int(got["kites_run_opts.time_kernels"]) == capi.RunOpts.time_kernels.offset
     assert int(got["kites_run_stats.pull_kernel_bytes"]) == capi.RunStats.pull_kernel_bytes.offset
     assert int(got["kites_run_stats.iter_edges"]) == capi.RunStats.iter_edges.offset
+    assert int(got["kites_run_stats.pull_dense_bytes"]) == capi.RunStats.pull_dense_bytes.offset
+    assert int(got["kites_csc_view.offsets64"]) == capi.CscView.offsets64.offset
 
 
 def test_default_opts():
