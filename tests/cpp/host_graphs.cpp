@@ -4,6 +4,9 @@
 //   host_graphs csr <edges> <vpg> <source> <out>
 //       kites::graph_csr<unsigned,unsigned>(file, f, vpg, edge_list_s_d):
 //       V, R, C, E, vBitmap words, dir_R, dir_C.
+//   host_graphs undir <edges> 1 <source> <out>
+//       kites::graph_csr<unsigned,unsigned>(file, f, edge_list_s_d, undirected,
+//       incomplete): the same arrays (dir_R, dir_C empty).
 //   host_graphs mip <edges> <cr> <source> <out>
 //       kites::graph_csr_mipmapped<unsigned,unsigned>(file, f, cr):
 //       V, R, C, E, vBitmap words, mipmap words.
@@ -49,9 +52,15 @@ int main(int argc, char **argv) {
   FILE *f = std::fopen(argv[5], "wb");
   if (!f) return 3;
   try {
-    if (mode == "csr") {
-      kites::graph_csr<unsigned, unsigned> g(argv[2], preprocess<unsigned, unsigned>, param,
-                                             kites::input_graph_form::edge_list_s_d);
+    if (mode == "csr" || mode == "undir") {
+      kites::graph_csr<unsigned, unsigned> g =
+          mode == "csr"
+              ? kites::graph_csr<unsigned, unsigned>(argv[2], preprocess<unsigned, unsigned>, param,
+                                                     kites::input_graph_form::edge_list_s_d)
+              : kites::graph_csr<unsigned, unsigned>(argv[2], preprocess<unsigned, unsigned>,
+                                                     kites::input_graph_form::edge_list_s_d,
+                                                     kites::graph_property::undirected,
+                                                     kites::edge_list_expression::incomplete);
       const uint64_t hdr[7] = {g.V.size(), g.R.size(), g.C.size(), g.E.size(),
                                g.vBitmap.size(), g.dir_R.size(), g.dir_C.size()};
       put(f, hdr, 7);

@@ -1,8 +1,9 @@
 """The host-side construction of the kites:: C++ front-end, on the CPU.
 
-tests/cpp/host_graphs.cpp builds kites::graph_csr (vertex groups 1, 2, 4, 8)
-and kites::graph_csr_mipmapped (block sizes 1, 3, 32, 100) from the
-config-1 edge list with g++, linked against host-memory stand-ins for the
+tests/cpp/host_graphs.cpp builds kites::graph_csr (vertex groups 1 to 64,
+directed and undirected) and kites::graph_csr_mipmapped (block sizes 1, 3,
+32, 100) from the config-1 edge list and the reference example's Wiki-Vote
+file with g++, linked against host-memory stand-ins for the
 four CUDA runtime calls the host buffers make (tests/cpp/host_runtime_stub.cpp),
 and every array must hash to the golden value the reference's own classes
 produced (tests/golden/make_golden.py)."""
@@ -44,8 +45,9 @@ def cfg1_file(cfg1_edges, tmp_path_factory):
     return str(path)
 
 
-def dump(tool, mode, edges, param, out):
-    subprocess.run([tool, mode, edges, str(param), "0", str(out)], check=True, capture_output=True)
+def dump(tool, mode, edges, param, out, source=0):
+    subprocess.run([tool, mode, edges, str(param), str(source), str(out)], check=True,
+                   capture_output=True)
     with open(out, "rb") as f:
         counts = [int(x) for x in np.frombuffer(f.read(56), np.uint64)]
         return [np.frombuffer(f.read(4 * k), np.uint32) for k in counts[:6 if mode == "mip" else 7]], counts
@@ -62,3 +64,35 @@ def test_graph_csr_mipmapped_matches_reference(tool, cfg1_file, golden, tmp_path
     (V, R, C, E, bits, mip), counts = dump(tool, "mip", cfg1_file, cr, tmp_path / "d.bin")
     assert counts[6] == golden["meta"]["cfg1_mipmap_dim"][str(cr)]
     assert sha(V, R, C, E, bits, mip) == bytes(golden[f"cfg1_mipmap_cr{cr}"])
+
+
+@pytest.mark.parametrize("vpg", [1, 2, 4, 8, 32, 64])
+def test_graph_csr_matches_reference_wiki(tool, golden, has_reference, tmp_path, vpg):
+    """The reference example's graph (Wiki-Vote, source 30, INF 2^30 - 1,
+    weights (s + 1)(d + 2) % 127) at every vertex-group size the reference
+    allows."""
+    if not has_reference:
+        pytest.skip("reference example file not present")
+    from conftest import WIKI
+    (V, R, C, E, bits, dR, dC), _ = dump(tool, "csr", WIKI, vpg, tmp_path / "d.bin", source=30)
+    assert sha(R, C, E, V, bits, dR, dC) == bytes(golden[f"wiki_struct_vpg{vpg}"])
+
+
+def test_graph_csr_undirected_matches_reference_wiki(tool, golden, has_reference, tmp_path):
+    if not has_reference:
+        pytest.skip("reference example file not present")
+    from conftest import WIKI
+    (V, R, C, E, bits, dR, dC), _ = dump(tool, "undir", WIKI, 1, tmp_path / "d.bin", source=30)
+    assert dR.size == 0 and dC.size == 0 and not bits.any()
+    assert sha(R, C, E, V, bits, dR, dC) == bytes(golden["wiki_undir_struct"])
+
+
+@pytest.mark.parametrize("cr", [1, 3, 32, 100])
+def test_graph_csr_mipmapped_matches_reference_wiki(tool, golden, has_reference, tmp_path, cr):
+    if not has_reference:
+        pytest.skip("reference example file not present")
+    from conftest import WIKI
+    (V, R, C, E, bits, mip), counts = dump(tool, "mip", WIKI, cr, tmp_path / "d.bin", source=30)
+    assert counts[6] == golden["meta"]["wiki"]["mipmap_dim"][str(cr)]
+    assert sha(V, R, C, E, bits, mip) == bytes(golden[f"wiki_mipmap_cr{cr}"])
+
