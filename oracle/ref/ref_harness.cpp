@@ -15,6 +15,10 @@
 //       ratio cr from an edge-list file and the same pre-processing
 //       function (SSSP values); dumps V, R, C, E, the block frontier and the
 //       block mipmap (kites/graph/graph_csr_mipmapped.hpp:40-78).
+//   save <edgelist> <vpg> <source> <out>
+//       the directed kites::graph_csr of `build` (SSSP values) written in the
+//       reference's prepared text format by kites::io::save_to_file
+//       (kites/io/graph_output.cuh:23-31).
 //   csc <in> <sssp_wrap|sssp_sat|bfs|cc> <out> [max_seconds]
 //       Reads a binary CSC and runs the reference's sanity_check loop on it
 //       with the four user functions of the chosen operator; dumps V and the
@@ -24,6 +28,7 @@
 // the fixed-point loop are the reference's code, included unmodified.
 #include "kites/graph/sanity_check.cuh"
 #include "kites/graph/graph_csr_mipmapped.hpp"
+#include "kites/io/graph_output.cuh"
 
 #include <chrono>
 #include <cstdint>
@@ -165,6 +170,17 @@ int run_mipmap(int argc, char **argv) {
   return 0;
 }
 
+int run_save(int argc, char **argv) {
+  if (argc < 6) return 2;
+  const unsigned vpg = static_cast<unsigned>(atoi(argv[3]));
+  g_source = static_cast<unsigned>(strtoul(argv[4], nullptr, 10));
+  g_label_init = false;
+  kites::graph_csr<unsigned, unsigned> g(argv[2], harness_preprocess<unsigned, unsigned>, vpg,
+                                         kites::input_graph_form::edge_list_s_d);
+  kites::io::save_to_file(g, std::string(argv[5]));
+  return 0;
+}
+
 int run_csc(int argc, char **argv) {
   if (argc < 5) return 2;
   std::string op = argv[3];
@@ -227,6 +243,7 @@ int main(int argc, char **argv) {
     if (argc >= 2 && std::string(argv[1]) == "build") return run_build(argc, argv);
     if (argc >= 2 && std::string(argv[1]) == "csc") return run_csc(argc, argv);
     if (argc >= 2 && std::string(argv[1]) == "mipmap") return run_mipmap(argc, argv);
+    if (argc >= 2 && std::string(argv[1]) == "save") return run_save(argc, argv);
   } catch (const std::exception &e) {
     fprintf(stderr, "%s\n", e.what());
     return 4;

@@ -7,6 +7,10 @@
 //   host_graphs undir <edges> 1 <source> <out>
 //       kites::graph_csr<unsigned,unsigned>(file, f, edge_list_s_d, undirected,
 //       incomplete): the same arrays (dir_R, dir_C empty).
+//   host_graphs save <edges> <vpg> <source> <out>
+//       kites::io::save_to_file of the directed graph_csr (prepared text).
+//   host_graphs load <prepared> 1 <source> <out>
+//       kites::graph_csr<unsigned,unsigned>(prepared file): the csr arrays.
 //   host_graphs mip <edges> <cr> <source> <out>
 //       kites::graph_csr_mipmapped<unsigned,unsigned>(file, f, cr):
 //       V, R, C, E, vBitmap words, mipmap words.
@@ -22,6 +26,7 @@
 
 #include "kites/graph/graph_csr.h"
 #include "kites/graph/graph_csr_mipmapped.hpp"
+#include "kites/io/graph_output.cuh"
 
 namespace {
 
@@ -49,12 +54,24 @@ int main(int argc, char **argv) {
   const std::string mode = argv[1];
   const unsigned param = static_cast<unsigned>(std::atoi(argv[3]));
   g_source = static_cast<unsigned>(std::strtoul(argv[4], nullptr, 10));
+  if (mode == "save") {
+    try {
+      kites::graph_csr<unsigned, unsigned> g(argv[2], preprocess<unsigned, unsigned>, param,
+                                             kites::input_graph_form::edge_list_s_d);
+      kites::io::save_to_file(g, std::string(argv[5]));
+    } catch (const std::exception &e) {
+      std::fprintf(stderr, "%s\n", e.what());
+      return 4;
+    }
+    return 0;
+  }
   FILE *f = std::fopen(argv[5], "wb");
   if (!f) return 3;
   try {
-    if (mode == "csr" || mode == "undir") {
+    if (mode == "csr" || mode == "undir" || mode == "load") {
       kites::graph_csr<unsigned, unsigned> g =
-          mode == "csr"
+          mode == "load" ? kites::graph_csr<unsigned, unsigned>(std::string(argv[2]))
+          : mode == "csr"
               ? kites::graph_csr<unsigned, unsigned>(argv[2], preprocess<unsigned, unsigned>, param,
                                                      kites::input_graph_form::edge_list_s_d)
               : kites::graph_csr<unsigned, unsigned>(argv[2], preprocess<unsigned, unsigned>,

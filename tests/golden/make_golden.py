@@ -87,6 +87,16 @@ def run_mipmap(edge_file, cr, source):
     return dim, sha(*arrays)
 
 
+def run_save(edge_file, vpg, source):
+    """sha256 of the reference's prepared text file (io::save_to_file)."""
+    with tempfile.TemporaryDirectory() as td:
+        out = os.path.join(td, "prepared.txt")
+        subprocess.run([HARNESS, "save", edge_file, str(vpg), str(source), out], check=True,
+                       capture_output=True)
+        with open(out, "rb") as f:
+            return hashlib.sha256(f.read()).hexdigest()
+
+
 def run_csc(R, C, E, V, op):
     with tempfile.TemporaryDirectory() as td:
         inp, out = os.path.join(td, "in.bin"), os.path.join(td, "out.bin")
@@ -158,6 +168,8 @@ def main(argv=None):
             dv = run_build(ef, vpg, 0)
             g[f"cfg1_struct_vpg{vpg}"] = np.frombuffer(bytes.fromhex(struct_hash(dv)),
                                                        np.uint8)
+        # The prepared text format (kites/io/graph_output.cuh:23-31).
+        g["cfg1_prepared_sha"] = np.frombuffer(bytes.fromhex(run_save(ef, 1, 0)), np.uint8)
         meta["cfg1_mipmap_dim"] = {}
         for cr in MIPMAP_CRS:
             dim, h = run_mipmap(ef, cr, 0)

@@ -96,3 +96,21 @@ def test_graph_csr_mipmapped_matches_reference_wiki(tool, golden, has_reference,
     assert counts[6] == golden["meta"]["wiki"]["mipmap_dim"][str(cr)]
     assert sha(V, R, C, E, bits, mip) == bytes(golden[f"wiki_mipmap_cr{cr}"])
 
+
+
+def test_prepared_format_matches_reference(tool, cfg1_file, golden, tmp_path):
+    """kites::io::save_to_file writes the reference's prepared text format
+    byte for byte (kites/io/graph_output.cuh:23-31)."""
+    out = tmp_path / "prepared.txt"
+    subprocess.run([tool, "save", cfg1_file, "1", "0", str(out)], check=True, capture_output=True)
+    assert hashlib.sha256(out.read_bytes()).digest() == bytes(golden["cfg1_prepared_sha"])
+
+
+def test_prepared_format_round_trip(tool, cfg1_file, golden, tmp_path):
+    """graph_csr(prepared file) reads back the graph that was saved
+    (kites/graph/graph_csr.h:112-166)."""
+    prepared = tmp_path / "prepared.txt"
+    subprocess.run([tool, "save", cfg1_file, "1", "0", str(prepared)], check=True,
+                   capture_output=True)
+    (V, R, C, E, bits, dR, dC), _ = dump(tool, "load", str(prepared), 1, tmp_path / "d.bin")
+    assert sha(R, C, E, V, bits, dR, dC) == bytes(golden["cfg1_struct_vpg1"])
