@@ -11,6 +11,11 @@
 //       kites::io::save_to_file of the directed graph_csr (prepared text).
 //   host_graphs load <prepared> 1 <source> <out>
 //       kites::graph_csr<unsigned,unsigned>(prepared file): the csr arrays.
+//   host_graphs check <edges> <vpg> <source> <values>
+//       kites::sanity_check over the directed graph_csr with the reference
+//       example's four functions (wrap-around add, min, less-than) against
+//       the uint32 values in the binary file <values>; exit status 0 iff it
+//       passes (its report goes to stdout).
 //   host_graphs mip <edges> <cr> <source> <out>
 //       kites::graph_csr_mipmapped<unsigned,unsigned>(file, f, cr):
 //       V, R, C, E, vBitmap words, mipmap words.
@@ -26,6 +31,7 @@
 
 #include "kites/graph/graph_csr.h"
 #include "kites/graph/graph_csr_mipmapped.hpp"
+#include "kites/graph/sanity_check.cuh"
 #include "kites/io/graph_output.cuh"
 
 namespace {
@@ -54,6 +60,28 @@ int main(int argc, char **argv) {
   const std::string mode = argv[1];
   const unsigned param = static_cast<unsigned>(std::atoi(argv[3]));
   g_source = static_cast<unsigned>(std::strtoul(argv[4], nullptr, 10));
+  if (mode == "check") {
+    try {
+      kites::graph_csr<unsigned, unsigned> g(argv[2], preprocess<unsigned, unsigned>, param,
+                                             kites::input_graph_form::edge_list_s_d);
+      kites::host_pinned_buffer<unsigned> want(g.get_num_vertices());
+      FILE *vf = std::fopen(argv[5], "rb");
+      if (!vf) return 3;
+      const size_t got = std::fread(want.get_ptr(), sizeof(unsigned), want.size(), vf);
+      std::fclose(vf);
+      if (got != want.size()) return 3;
+      auto initF = [](unsigned &loc, unsigned &glob) { loc = glob; };
+      auto compF = [](unsigned &partial, unsigned srcV, unsigned *e) { partial = srcV + *e; };
+      auto redF = [](unsigned &lhs, unsigned &rhs) { if (lhs > rhs) lhs = rhs; };
+      auto updF = [](unsigned &nv, unsigned ov) { return nv < ov; };
+      const bool ok = kites::sanity_check(g.get_num_vertices(), g.V, g.R, g.C, g.E, want, initF,
+                                          compF, redF, updF);
+      return ok ? 0 : 5;
+    } catch (const std::exception &e) {
+      std::fprintf(stderr, "%s\n", e.what());
+      return 4;
+    }
+  }
   if (mode == "save") {
     try {
       kites::graph_csr<unsigned, unsigned> g(argv[2], preprocess<unsigned, unsigned>, param,

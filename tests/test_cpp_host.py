@@ -14,6 +14,8 @@ import subprocess
 import numpy as np
 import pytest
 
+from oracle import oracle as O
+
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 CPP = os.path.join(ROOT, "tests", "cpp")
 
@@ -114,3 +116,38 @@ def test_prepared_format_round_trip(tool, cfg1_file, golden, tmp_path):
                    capture_output=True)
     (V, R, C, E, bits, dR, dC), _ = dump(tool, "load", str(prepared), 1, tmp_path / "d.bin")
     assert sha(R, C, E, V, bits, dR, dC) == bytes(golden["cfg1_struct_vpg1"])
+
+
+def test_sanity_check_agrees_with_reference_wiki(tool, golden, has_reference, tmp_path):
+    """kites::sanity_check (the reference's CPU verifier, kites/graph/sanity_check.cuh:13-59)
+    passes on the reference's fixed point of the example graph after the same number of
+    Gauss-Seidel sweeps, and reports the first mismatch of a perturbed result."""
+    if not has_reference:
+        pytest.skip("reference example file not present")
+    from conftest import WIKI
+    want = golden["wiki_sssp"].astype(np.uint32)
+    vf = tmp_path / "v.bin"
+    vf.write_bytes(want.tobytes())
+    r = subprocess.run([tool, "check", WIKI, "1", "30", str(vf)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "SANITY CHECK: PASSED" in r.stdout
+    sweeps = golden["meta"]["wiki"]["sweeps"]
+    assert f"performed {sweeps} iterations" in r.stdout
+    bad = want.copy()
+    i = int(np.flatnonzero(bad < 1000)[3])
+    bad[i] += 1
+    vf.write_bytes(bad.tobytes())
+    r = subprocess.run([tool, "check", WIKI, "1", "30", str(vf)], capture_output=True, text=True)
+    assert r.returncode == 5 and f"MISMATCH at index {i}" in r.stdout
+
+
+def test_sanity_check_agrees_with_oracle_cfg1(tool, cfg1_file, tmp_path):
+    vals = np.loadtxt(cfg1_file, dtype=np.int64).astype(np.uint32)
+    hg = O.build_host_graph(vals[:, 0], vals[:, 1], vals[:, 2], init="source", source=0,
+                            inf=1073741823)
+    want, _ = O.sanity_check(hg, op=O.OP_SSSP_WRAP)
+    vf = tmp_path / "v.bin"
+    vf.write_bytes(np.asarray(want, np.uint32).tobytes())
+    r = subprocess.run([tool, "check", cfg1_file, "1", "0", str(vf)], capture_output=True,
+                       text=True)
+    assert r.returncode == 0 and "SANITY CHECK: PASSED" in r.stdout
