@@ -12,7 +12,9 @@ enum {
   WARP_SIZE_SHIFT = 5
 };
 
-// launch::async is accepted and treated as sync, as in the reference.
+// process<launch::async> runs like launch::sync (the reference's process
+// template never reads its launch mode); copyMem<T, launch::async> enqueues
+// its copy without waiting.
 enum class launch { sync = true, async = false };
 enum class operation_mode { iterative = true, frontier_based = false };
 enum class input_graph_form { edge_list_s_d = true, edge_list_d_s = false };

@@ -14,9 +14,17 @@
 
 namespace kites {
 
+// launch::sync blocks and returns the copy's wall time in ms; launch::async
+// enqueues the copy on the default stream and returns 0 at once (the caller
+// synchronises), as the reference's overload does.
 template <class T, launch lMode = launch::sync>
 double copyMem(uva_buffer<T> &dst, uva_buffer<T> &src, std::size_t length,
                std::size_t dstOffst = 0, std::size_t srcOffst = 0) {
+  if (lMode == launch::async) {
+    CUDAErrorCheck(cudaMemcpyAsync(dst.get_ptr() + dstOffst, src.get_ptr() + srcOffst,
+                                   length * sizeof(T), cudaMemcpyDefault));
+    return 0;
+  }
   auto t0 = std::chrono::steady_clock::now();
   CUDAErrorCheck(cudaMemcpy(dst.get_ptr() + dstOffst, src.get_ptr() + srcOffst,
                             length * sizeof(T), cudaMemcpyDefault));

@@ -59,8 +59,17 @@ struct run_counters {
   unsigned long long changed;         // rows marked changed by the pull/push kernels
   unsigned long long last_changed;
   uint32_t sel;                       // strategy class picked for the next iteration
-  uint32_t error;                     // a kernel's self-check failed (bad staged index)
+  uint32_t error;                     // kErr* bits: why a kernel stopped the run
 };
+
+// run_counters::error bits, set with atomicOr; any bit ends the loop.
+constexpr uint32_t kErrIndex = 1u;    // an index read during the run was out of range
+                                      // (the access was skipped)
+constexpr uint32_t kErrWait = 2u;     // a bounded wait on a TMA copy gave up
+
+__device__ __forceinline__ void raise_error(run_counters *c, uint32_t bit) {
+  atomicOr(&c->error, bit);
+}
 
 // ---- warp primitives ---------------------------------------------------
 
@@ -74,6 +83,15 @@ __device__ __forceinline__ uint32_t warp_inclusive_scan(uint32_t x) {
     uint32_t y = __shfl_up_sync(kFull, x, d);
     if (lane >= (uint32_t)d) x += y;
   }
+  return x;
+}
+
+// Sum of a 64-bit value over the warp (every lane gets it).  Per-lane edge
+// and degree counts can pass 2^32 on graphs with 64-bit offsets, so they
+// are never narrowed before the reduction.
+__device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long x) {
+#pragma unroll
+  for (int d = 16; d; d >>= 1) x += __shfl_xor_sync(kFull, x, d);
   return x;
 }
 

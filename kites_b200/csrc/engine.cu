@@ -59,6 +59,18 @@ int dev_alloc(kites_engine *eng, void **p, size_t bytes) {
   return KITES_OK;
 }
 
+// Status of a run that a kernel stopped (run_counters::error bits).  A wait
+// that gave up is a timeout; an out-of-range index read during the run means
+// the device arrays no longer hold what the upload validated.
+int run_error(uint32_t err) {
+  if (err & kErrWait)
+    return fail(KITES_ERR_TIMEOUT,
+                "a bounded wait on a TMA row copy gave up (error bits 0x%x)", err);
+  return fail(KITES_ERR_CUDA,
+              "a kernel read an out-of-range vertex or edge index and skipped it "
+              "(error bits 0x%x)", err);
+}
+
 int graph_alloc(kites_graph *g, void **p, size_t bytes) {
   KITES_TRY(dev_alloc(g->eng, p, bytes));
   g->owned.push_back(*p);
@@ -631,7 +643,7 @@ int run_plain(kites_graph *g, const kites_run_opts &o, kites_run_stats *st) {
     st->kernel_launches += launches;
     if (o.record_iterations) KITES_TRY(record_iterations(g, c, KITES_STRATEGY_PLAIN, st));
   }
-  if (c.error) return fail(KITES_ERR_CUDA, "a kernel self-check failed (staged index)");
+  if (c.error) return run_error(c.error);
   if (c.timed_out)
     return fail(KITES_ERR_TIMEOUT, "no fixed point after %llu iterations",
                 (unsigned long long)c.iterations);
@@ -836,7 +848,7 @@ int run_flex(kites_graph *g, const kites_run_opts &o, kites_run_stats *st) {
     if (o.record_iterations) KITES_TRY(record_iterations(g, c, strategy, st));
     st->host_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   }
-  if (c.error) return fail(KITES_ERR_CUDA, "a kernel self-check failed (staged index)");
+  if (c.error) return run_error(c.error);
   if (c.timed_out)
     return fail(KITES_ERR_TIMEOUT, "no fixed point after %llu iterations",
                 (unsigned long long)c.iterations);
@@ -1063,7 +1075,7 @@ int run_auto(kites_graph *g, const kites_run_opts &o, kites_run_stats *st) {
     }
     st->host_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   }
-  if (c.error) return fail(KITES_ERR_CUDA, "a kernel self-check failed (staged index)");
+  if (c.error) return run_error(c.error);
   if (c.timed_out)
     return fail(KITES_ERR_TIMEOUT, "no fixed point after %llu iterations",
                 (unsigned long long)c.iterations);
@@ -1354,7 +1366,7 @@ int run_batch(kites_graph *g, const uint32_t *sources, uint32_t *dist_out,
     if (o.record_iterations) KITES_TRY(record_iterations(g, c, KITES_STRATEGY_PLAIN, st));
     st->host_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   }
-  if (c.error) return fail(KITES_ERR_CUDA, "a kernel self-check failed (staged index)");
+  if (c.error) return run_error(c.error);
   if (c.timed_out)
     return fail(KITES_ERR_TIMEOUT, "no fixed point after %llu iterations",
                 (unsigned long long)c.iterations);

@@ -203,7 +203,7 @@ __global__ void __launch_bounds__(kTmaWarps * 32)
     const bool got = mbar_wait(&mt.bar[b], (phase >> b) & 1u);
     if (!__all_sync(kFull, got)) {
       ok = false;
-      if (lane == 0) a.ctr->error = 1u;
+      if (lane == 0) raise_error(a.ctr, kErrWait);
       return;
     }
     phase ^= 1u << b;
@@ -291,7 +291,7 @@ __global__ void __launch_bounds__(kTmaWarps * 32)
             s_src = __ldcs(a.g.C + e);
             s_w = kW ? __ldcs(a.E + e) : 0u;
             if (s_src >= a.g.n_rows) {  // out of range: never gather it
-              a.ctr->error = 1u;
+              raise_error(a.ctr, kErrIndex);
               s_skip = true;
               s_src = s_row;
             }

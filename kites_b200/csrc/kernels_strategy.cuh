@@ -51,8 +51,7 @@ __global__ void k_compact_queue(const uint32_t *__restrict__ U, uint64_t nwords,
     }
     cnt += c;
   }
-  cnt = __reduce_add_sync(kFull, (uint32_t)cnt);
-  odeg = __reduce_add_sync(kFull, (uint32_t)odeg);
+  odeg = warp_sum_u64(odeg);
   if (lane == 0 && odeg) atomicAdd(&ctr->out_edges, odeg);
   (void)cnt;
 }
@@ -180,8 +179,8 @@ __global__ void __launch_bounds__(kBlock) k_pull_tpv(pull_tpv_args<OffT> a) {
       a.ctr->update_flag = 1u;
     }
   }
-  n_act = __reduce_add_sync(kFull, (uint32_t)n_act);
-  n_edges = __reduce_add_sync(kFull, (uint32_t)n_edges);
+  n_act = warp_sum_u64(n_act);
+  n_edges = warp_sum_u64(n_edges);
   if (lane == 0) {
     if (n_act) atomicAdd(&a.ctr->active, n_act);
     if (n_edges) atomicAdd(&a.ctr->edges, n_edges);

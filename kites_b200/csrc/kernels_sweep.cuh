@@ -121,7 +121,7 @@ __global__ void __launch_bounds__(kSweepThreads, kSweepMinBlocks) k_sweep(sweep_
 #pragma unroll
       for (int k = 0; k < kEdgesPerThread; ++k) mx = max(mx, max(row[k], src[k]));
       const bool bad = mx >= a.n_rows || row[0] > row[kEdgesPerThread - 1];
-      if (bad) a.ctr->error = 1u;  // never index with an id out of range
+      if (bad) raise_error(a.ctr, kErrIndex);  // never index with an id out of range
       uint32_t val[kEdgesPerThread], fw[kEdgesPerThread];
       uint32_t w_first = kFull, w_last = kFull;
       if (MODE == kRowFilter && !bad) {
@@ -203,7 +203,7 @@ __global__ void __launch_bounds__(kSweepThreads, kSweepMinBlocks) k_sweep(sweep_
     for (int k = 0; k < kEdgesPerThread; ++k) {
       live[k] = row[k] != kNoRow;
       if (live[k] && (src[k] >= a.n_rows || row[k] >= a.n_rows)) {
-        a.ctr->error = 1u;  // never index with an id out of range
+        raise_error(a.ctr, kErrIndex);  // never index with an id out of range
         live[k] = false;
         row[k] = kNoRow;
       }
@@ -337,7 +337,7 @@ __global__ void __launch_bounds__(kSweepThreads, kSweepMinBlocks)
 #pragma unroll
       for (int k = 0; k < kEdgesPerThread; ++k) mx = max(mx, max(row[k], src[k]));
       const bool bad = mx >= a.n_rows || row[0] > row[kEdgesPerThread - 1];
-      if (bad) a.ctr->error = 1u;  // never index with an id out of range
+      if (bad) raise_error(a.ctr, kErrIndex);  // never index with an id out of range
       uint32_t hit[kEdgesPerThread], cand[kEdgesPerThread];
 #pragma unroll
       for (int k = 0; k < kEdgesPerThread; ++k) {
@@ -390,7 +390,7 @@ __global__ void __launch_bounds__(kSweepThreads, kSweepMinBlocks)
     for (int k = 0; k < kEdgesPerThread; ++k) {
       if (row[k] == kNoRow) continue;
       if (src[k] >= a.n_rows || row[k] >= a.n_rows) {
-        a.ctr->error = 1u;  // never index with an id out of range
+        raise_error(a.ctr, kErrIndex);  // never index with an id out of range
         continue;
       }
       if (!((a.U[src[k] >> 5] >> (src[k] & 31u)) & 1u)) continue;
@@ -447,7 +447,7 @@ __global__ void __launch_bounds__(kSweepThreads) k_activate_sweep(sweep_args<Off
 #pragma unroll
       for (int k = 0; k < kEdgesPerThread; ++k) mx = max(mx, max(row[k], src[k]));
       const bool bad = mx >= a.n_rows || row[0] > row[kEdgesPerThread - 1];
-      if (bad) a.ctr->error = 1u;
+      if (bad) raise_error(a.ctr, kErrIndex);
       uint32_t hit[kEdgesPerThread];
 #pragma unroll
       for (int k = 0; k < kEdgesPerThread; ++k) {
@@ -487,7 +487,7 @@ __global__ void __launch_bounds__(kSweepThreads) k_activate_sweep(sweep_args<Off
 #pragma unroll
     for (int k = 0; k < kEdgesPerThread; ++k) {
       if (row[k] != kNoRow && (src[k] >= a.n_rows || row[k] >= a.n_rows)) {
-        a.ctr->error = 1u;
+        raise_error(a.ctr, kErrIndex);
         row[k] = kNoRow;
       }
       uw[k] = row[k] != kNoRow ? a.U[src[k] >> 5] : 0u;

@@ -9,7 +9,9 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
-REFERENCE = "/root/reference"
+from oracle.reference_dir import REFERENCE_DIR, reference_dir  # noqa: E402
+
+REFERENCE = REFERENCE_DIR
 WIKI = os.path.join(REFERENCE, "examples", "Sample-Graph-Wiki-Vote.txt")
 
 
@@ -28,7 +30,7 @@ def golden():
 
 @pytest.fixture(scope="session")
 def has_reference():
-    return os.path.isdir(os.path.join(REFERENCE, "kites"))
+    return reference_dir() is not None
 
 
 @pytest.fixture(scope="session")

@@ -1,6 +1,6 @@
 """Regenerates tests/golden/golden.npz from farkhor/KiTES's OWN host code.
 
-    python tests/golden/make_golden.py [--ref /root/reference]
+    python tests/golden/make_golden.py [--ref <reference tree>]
 
 Needs the reference tree (only in the development container) and the
 harness built from it (`make -C oracle ref`).  Every vector here comes out
@@ -26,6 +26,7 @@ sys.path.insert(0, ROOT)
 
 from kites_b200 import capi  # noqa: E402  (generators only)
 from oracle import oracle as O  # noqa: E402
+from oracle.reference_dir import REFERENCE_DIR  # noqa: E402
 
 HARNESS = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
 OUT = os.path.join(ROOT, "tests", "golden", "golden.npz")
@@ -124,7 +125,8 @@ def write_edges(path, src, dst, w=None):
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=REFERENCE_DIR,
+                    help="reference tree (default: KITES_REFERENCE_DIR)")
     args = ap.parse_args(argv)
     subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), f"REF={args.ref}", "all"],
                    check=True, capture_output=True)

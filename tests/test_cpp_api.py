@@ -12,6 +12,7 @@ import pytest
 
 from kites_b200 import capi
 from oracle import oracle as O
+from oracle.reference_dir import REFERENCE_DIR as REFERENCE
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 NVCC = "/usr/local/cuda/bin/nvcc"
@@ -34,7 +35,7 @@ def test_reference_example_compiles_unchanged(has_reference, tmp_path):
         pytest.skip("reference tree not present")
     ex = tmp_path / "examples"
     ex.mkdir()
-    shutil.copy("/root/reference/examples/sssp_basic_single_device.cu", ex)
+    shutil.copy(os.path.join(REFERENCE, "examples", "sssp_basic_single_device.cu"), ex)
     os.symlink(os.path.join(ROOT, "include", "kites"), tmp_path / "kites")
     nvcc("sssp_basic_single_device.cu", str(ex / "a.out"), cwd=str(ex))
     assert (ex / "a.out").exists()

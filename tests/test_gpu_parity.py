@@ -243,14 +243,15 @@ def test_repeated_runs_and_pool_reuse(engine, cfg1_edges):
 @pytest.mark.parametrize("k", [32, 64, 128, 256])
 @pytest.mark.parametrize("device_loop", [0, 1])
 def test_batch_gather_modes_agree(engine, k, device_loop):
-    """TMA row gathers (default for K >= 32) and register loads give the same
-    V x K distances, run after run, on one graph."""
+    """TMA row gathers (gather mode 1, K >= 32) and register loads (mode 0,
+    the default) give the same V x K distances, run after run, on one graph."""
     n = 1 << 14
     s, d, w = capi.gen_rmat(14, 16 << 14, seed=31)
     R, C, E = capi.csc_from_edges(n, s, d, w)
     g = capi.Graph(engine, R, C, E)
     srcs = np.random.default_rng(100 + k).choice(n, size=k, replace=False).astype(np.uint32)
     o = capi.default_opts(device_loop=device_loop)
+    g.set_batch_gather(1)
     tma, st = g.sssp_batch(srcs, opts=o)
     g.set_batch_gather(0)
     loads, _ = g.sssp_batch(srcs, opts=o)
