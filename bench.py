@@ -18,9 +18,18 @@ Multi-GPU: replicas only -- each rank runs its own sources on its own copy
 of the graph (weak scaling); torch.distributed carries only the barrier and
 the max-over-ranks of the timings.
 
+Input: the graph is read from a binary CSC file (kites_csc_save's layout)
+in $KITES_GRAPH_CACHE (default: <tmp>/kites_graph_cache) when one with the
+same description exists, and generated and written there otherwise, so that
+a 268M-edge graph is built once per machine.
+
 --impl reference times farkhor/KiTES's own CPU vertex-centric loop
 (kites::sanity_check, compiled from the reference headers into
-oracle/_ref/libref_harness.so) on a bounded sample of the workload.
+oracle/_ref/libref_harness.so) on the same graph: each step is the SSSP of
+one of the workload's sources, and the steps run side by side, one per host
+thread.  That process reads or generates the graph through the oracle only
+(oracle/csc_file.py, the oracle's own generator) and never loads the
+library under test.
 """
 from __future__ import annotations
 
@@ -72,7 +81,8 @@ def parse():
                     help="skip kites_autotune (batch chunk size, sweep densities, TPV width) "
                          "before the warm-up")
     ap.add_argument("--seed", type=int, default=1)
-    ap.add_argument("--ref-sample-scale", type=int, default=20)
+    ap.add_argument("--ref-threads", type=int, default=0,
+                    help="host threads of the reference loop (0 = every core this process may use)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -83,14 +93,64 @@ def parse():
 # helpers
 # ---------------------------------------------------------------------------
 
+def graph_desc(scale, edge_factor, seed):
+    return (f"rmat scale={scale} m={edge_factor << scale} a,b,c=0.57,0.19,0.19 "
+            f"seed={seed} w=1..255 directed")
+
+
+def cache_path(scale, edge_factor, seed):
+    import tempfile
+    d = os.environ.get("KITES_GRAPH_CACHE") or os.path.join(tempfile.gettempdir(),
+                                                             "kites_graph_cache")
+    os.makedirs(d, exist_ok=True)
+    return os.path.join(d, f"rmat{scale}_ef{edge_factor}_seed{seed}.csc")
+
+
 def make_graph(scale, edge_factor, seed):
+    """The benchmark graph through the library: read from the CSC cache when
+    it holds this graph, else generated (kites_gen_rmat + kites_csc_from_edges)
+    and written there (kites_csc_save)."""
     from kites_b200 import capi
     n = 1 << scale
     m = edge_factor * n
-    s, d, w = capi.gen_rmat(scale, m, 0.57, 0.19, 0.19, seed, 1, 255)
-    R, C, E = capi.csc_from_edges(n, s, d, w)
-    outdeg = np.bincount(s, minlength=n).astype(np.uint64)
-    del s, d, w
+    path, desc = cache_path(scale, edge_factor, seed), graph_desc(scale, edge_factor, seed)
+    R = None
+    try:
+        if capi.csc_info(path)[4] == desc:
+            R, C, E = capi.csc_load(path)
+    except capi.KitesError:
+        R = None
+    if R is None:
+        s, d, w = capi.gen_rmat(scale, m, 0.57, 0.19, 0.19, seed, 1, 255)
+        R, C, E = capi.csc_from_edges(n, s, d, w)
+        del s, d, w
+        capi.csc_save(path, R, C, E, directed=True, desc=desc)
+    outdeg = np.bincount(C, minlength=n).astype(np.uint64)
+    return n, m, R, C, E, outdeg
+
+
+def make_graph_oracle(scale, edge_factor, seed):
+    """The same graph for the reference arm, through the oracle alone: read
+    with numpy (oracle/csc_file.py), or generated by the oracle's own
+    restatement of the generator rule and written to the same cache."""
+    from oracle import csc_file
+    from oracle import oracle as O
+    n = 1 << scale
+    m = edge_factor * n
+    path, desc = cache_path(scale, edge_factor, seed), graph_desc(scale, edge_factor, seed)
+    R = None
+    try:
+        R, C, E, _, got = csc_file.read(path)
+        if got != desc:
+            R = None
+    except (OSError, ValueError):
+        R = None
+    if R is None:
+        s, d, w = O.gen_rmat(scale, m, 0.57, 0.19, 0.19, seed, 1, 255)
+        R, C, E = O.csc_from_edges(n, s, d, w)
+        del s, d, w
+        csc_file.write(path, R, C, E, directed=True, desc=desc)
+    outdeg = np.bincount(C, minlength=n).astype(np.uint64)
     return n, m, R, C, E, outdeg
 
 
@@ -201,17 +261,6 @@ def barrier(world):
 # reference CPU arm
 # ---------------------------------------------------------------------------
 
-def ref_sample(scale, seed, sources=1):
-    """Bounded sample for the reference's single-thread loop: SSSP from
-    seeded sources on an R-MAT of `scale` with the same generator and
-    parameters as the benchmark graph."""
-    n, m, R, C, E, outdeg = make_graph(scale, 16, seed)
-    if R[-1] > 0xFFFFFFFF:
-        raise RuntimeError("reference loop takes 32-bit offsets")
-    srcs = pick_sources(outdeg, sources, seed)
-    return n, m, R.astype(np.uint32), C, E, outdeg, srcs
-
-
 @contextlib.contextmanager
 def reference_output_silenced():
     """The reference's loop (kites::sanity_check) prints its own report and
@@ -232,36 +281,48 @@ def reference_output_silenced():
         os.close(saved)
 
 
-def time_reference(lib, n, m, R32, C, E, outdeg, src):
-    V = np.full(n, 0xFFFFFFFF, np.uint32)
-    V[src] = 0
-    p = lambda a: a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
-    with reference_output_silenced():
-        secs = lib.ref_sanity_check_csc(0, n, m, p(V), p(R32), p(C), p(E))
-    if secs < 0:
-        raise RuntimeError("reference loop failed")
-    return secs, reached_edges(V, outdeg)
+def host_threads(requested=0):
+    return requested or len(os.sched_getaffinity(0))
 
 
 def load_ref_lib():
     if not os.path.exists(REF_LIB):
         return None
     lib = ctypes.CDLL(REF_LIB)
-    lib.ref_sanity_check_csc.restype = ctypes.c_double
-    lib.ref_sanity_check_csc.argtypes = [ctypes.c_int, ctypes.c_uint64, ctypes.c_uint64] + \
-        [ctypes.c_void_p] * 4
+    lib.ref_sssp_sources.restype = ctypes.c_double
+    lib.ref_sssp_sources.argtypes = [ctypes.c_uint64, ctypes.c_uint64] + [ctypes.c_void_p] * 4 + \
+        [ctypes.c_uint32, ctypes.c_uint32] + [ctypes.c_void_p] * 4
     return lib
 
 
-def ref_sample_text(scale, n, m):
-    return (f"single-source SSSP on R-MAT scale {scale} ({n} vertices, {m} edges, same "
-            f"generator and parameters as the benchmark graph), one seeded source per "
-            f"step, farkhor/KiTES kites::sanity_check loop, 1 thread")
+def time_reference(lib, n, m, R32, C, E, outdeg, sources, threads, want_dist=False):
+    """SSSP from each source by the reference's loop, `threads` sources side
+    by side.  Returns (wall seconds, reached edges per source, distances
+    n x len(sources) column-major or None)."""
+    src = np.ascontiguousarray(sources, dtype=np.uint32)
+    k = src.shape[0]
+    reached = np.zeros(k, np.uint64)
+    secs_each = np.zeros(k, np.float64)
+    dist = np.empty((k, n), np.uint32) if want_dist else None
+    od = np.ascontiguousarray(outdeg, dtype=np.uint64)
+    p = lambda a: None if a is None else a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
+    with reference_output_silenced():
+        secs = lib.ref_sssp_sources(n, m, p(R32), p(C), p(E), p(src), k, threads, p(od),
+                                    p(reached), p(secs_each), p(dist))
+    if secs < 0:
+        raise RuntimeError(f"reference loop failed ({secs})")
+    return secs, reached, dist
+
+
+def ref_sample_text(n, m, k, threads):
+    return (f"SSSP from {k} of the workload's sources on the same R-MAT graph ({n} vertices, "
+            f"{m} edges), one source per step, by farkhor/KiTES's own kites::sanity_check loop "
+            f"(single-threaded per source), {threads} sources side by side on {threads} host "
+            f"threads")
 
 
 def run_reference(args):
     world, rank, _ = dist_setup("gloo")
-    config = workload_config(args)
     if rank != 0:
         return 0
     lib = load_ref_lib()
@@ -270,24 +331,35 @@ def run_reference(args):
                           "unavailable": "oracle/_ref/libref_harness.so not built "
                                          "(needs the reference tree at build time)"}))
         return 0
-    n, m, R32, C, E, outdeg, srcs = ref_sample(args.ref_sample_scale, args.seed,
-                                               args.warmup + args.steps)
-    times, edges = [], []
-    for i in range(args.warmup + args.steps):
-        secs, me = time_reference(lib, n, m, R32, C, E, outdeg, int(srcs[i]))
-        if i >= args.warmup:
-            times.append(secs)
-            edges.append(me)
-    total_t = sum(times)
-    value = sum(edges) / total_t / 1e9
+    n, m, R, C, E, outdeg = make_graph_oracle(args.scale, args.edge_factor, args.seed)
+    if int(R[-1]) >= 1 << 31:
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "the reference loop masks bit 31 of row offsets"}))
+        return 0
+    R32 = R.astype(np.uint32)
+    del R
+    threads = host_threads(args.ref_threads)
+    srcs = pick_sources(outdeg, max(args.sources, args.steps + args.warmup), args.seed)
+    # Warm-up: W steps (sources) side by side, untimed; then exactly K steps,
+    # the first K of the workload's sources, timed from the first loop's
+    # start to the last one's end.
+    if args.warmup:
+        time_reference(lib, n, m, R32, C, E, outdeg, srcs[args.steps:args.steps + args.warmup],
+                       threads)
+    secs, reached, _ = time_reference(lib, n, m, R32, C, E, outdeg, srcs[:args.steps], threads)
+    value = float(reached.sum()) / secs / 1e9
+    config = dict(workload_config(args), mode="reference CPU loop", batch=1,
+                  sources_per_step=1, strategy="kites::sanity_check (Gauss-Seidel sweep)",
+                  threads=min(threads, args.steps), batch_gather=None)
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1e3 * total_t / len(times), "higher_is_better": True,
+        "ms_per_step": 1e3 * secs / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
         "config": config,
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
-                         "sample": ref_sample_text(args.ref_sample_scale, n, m)},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": min(threads, args.steps),
+                         "kind": "reference",
+                         "sample": ref_sample_text(n, m, args.steps, min(threads, args.steps))},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }))
@@ -322,7 +394,6 @@ def run_ours(args):
     n, m, R, C, E, outdeg = make_graph(args.scale, args.edge_factor, args.seed)
     eng = capi.Engine(local)
     g = capi.Graph(eng, R, C, E)
-    del C, E
     g.set_batch_gather(1 if args.batch_gather == "tma" else 0)
     stream = torch.cuda.ExternalStream(g.device_view().stream, device=device)
     srcs = pick_sources(outdeg, args.sources, args.seed, offset=rank)
@@ -478,15 +549,42 @@ def run_ours(args):
                "h2d_bytes_per_step": 4 * len(srcs),
                "d2h_bytes_per_step": 4 * n * len(srcs)}
 
+    # Correctness of what was timed, after the timed region: the distances of
+    # the first batch (or the first sources of --mode single), column for
+    # column bit-exact against the plain single-source kernel, and -- with
+    # the CPU baseline -- against farkhor/KiTES's own loop on the same
+    # sources, which is also the CPU baseline's timed sample.
+    first = groups[0] if args.mode == "batch" else srcs[:K]
+    got = np.empty((n, len(first)), np.uint32)
+    if args.mode == "batch":
+        capi._check(lib.kites_sssp_batch(eng._h, g._h, capi.OP_SSSP, capi._p(first), K,
+                                         capi._p(got), ctypes.byref(bopts), None))
+    else:
+        col = np.empty(n, np.uint32)
+        for j, s_ in enumerate(first):
+            got[:, j] = g.sssp(int(s_), out=col, opts=sopts)[0]
+    plain_cols = [0, len(first) - 1]
+    single = np.empty(n, np.uint32)
+    ok_plain = all(np.array_equal(got[:, j], g.sssp(int(first[j]), out=single)[0])
+                   for j in plain_cols)
+    checked = {"columns_vs_plain_kernel": len(plain_cols), "bit_exact_vs_plain": ok_plain}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         rlib = load_ref_lib()
-        if rlib is not None:
-            n2, m2, R32, C2, E2, od2, s2 = ref_sample(args.ref_sample_scale, args.seed, 1)
-            secs, me = time_reference(rlib, n2, m2, R32, C2, E2, od2, int(s2[0]))
-            cpu = {"value": me / secs / 1e9, "unit": UNIT, "cores": 1, "kind": "reference",
-                   "sample": ref_sample_text(args.ref_sample_scale, n2, m2) +
-                   f" ({secs:.2f} s)"}
+        if rlib is not None and int(R[-1]) < 1 << 31:
+            threads = host_threads(args.ref_threads)
+            k = min(threads, len(first))
+            secs, reached_ref, ref_dist = time_reference(
+                rlib, n, m, R.astype(np.uint32), C, E, outdeg, first[:k], threads,
+                want_dist=True)
+            ok_ref = all(np.array_equal(got[:, j], ref_dist[j]) for j in range(k))
+            checked.update(columns_vs_reference_loop=k, bit_exact_vs_reference=ok_ref)
+            cpu = {"value": float(reached_ref.sum()) / secs / 1e9, "unit": UNIT, "cores": k,
+                   "kind": "reference",
+                   "sample": ref_sample_text(n, m, k, k) + f" ({secs:.1f} s)"}
+    checked["ok"] = all(v for key, v in checked.items() if key.startswith("bit_exact"))
+    del got
 
     if rank == 0:
         line = {
@@ -520,6 +618,7 @@ def run_ours(args):
                                       "launches": d_launch, "peak_source": src_note}
                                      if d_ach is not None else None),
             "cpu_baseline": cpu,
+            "checked": checked,
         }
         print(json.dumps(line))
     g.close()

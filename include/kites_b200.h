@@ -222,7 +222,7 @@ int kites_sssp(kites_engine *eng, kites_graph *g, int op, uint32_t source,
                kites_run_stats *stats);
 
 /* Batched multi-source SSSP/BFS: K sources at once, distances in a
- * V x K vertex-major array (dist_out[v*K + k]); K <= 64. */
+ * V x K vertex-major array (dist_out[v*K + k]); K is 16, 32, 64, 128 or 256. */
 int kites_sssp_batch(kites_engine *eng, kites_graph *g, int op,
                      const uint32_t *sources, uint32_t k, uint32_t *dist_out,
                      const kites_run_opts *opts, kites_run_stats *stats);
@@ -317,9 +317,9 @@ int kites_autotune(kites_engine *eng, kites_graph *g, int op, const uint32_t *so
  * changed rows exceed dense_rows (0 = always, UINT64_MAX = never). */
 int kites_graph_set_density(kites_graph *g, uint64_t dense_edges, uint64_t dense_rows);
 /* How kites_sssp_batch fetches the K-wide source rows (no counterpart in the
- * reference, whose kernels run one source at a time): 1 (default) = TMA
- * tile::gather4 copies into shared memory when K >= 32, 0 = register loads.
- * Both give identical results. */
+ * reference, whose kernels run one source at a time): 0 (default) = 256-bit
+ * register loads, 1 = TMA tile::gather4 copies into shared memory when
+ * K >= 32.  Both give identical results. */
 int kites_graph_set_batch_gather(kites_graph *g, int mode);
 
 /* ---- synthetic graphs (host, deterministic, OpenMP) ------------------ */
@@ -351,6 +351,26 @@ int kites_csc_from_edges(uint64_t n_vertices, uint64_t n_edges,
                          const uint32_t *src, const uint32_t *dst,
                          const uint32_t *w, uint64_t *R, uint32_t *C,
                          uint32_t *E);
+
+/* ---- binary CSC files ------------------------------------------------
+ * The reference's prepared format is text, one value per line
+ * (kites/io/graph_output.cuh:23-38, read back by the graph_csr(file)
+ * constructor, kites/graph/graph_csr.h:112-166); these keep the same CSC
+ * (R, C, E) as raw arrays behind a 128-byte header, so that a large graph is
+ * built once and read back in seconds.  Layout: "KITESCSC", uint32 version 1,
+ * uint32 flags (1: edge values, 2: directed), uint64 n_vertices, uint64
+ * n_edges, uint64 0, char desc[88]; then R (n_vertices + 1 uint64), C and E
+ * (n_edges uint32 each).  A file is written under a temporary name and
+ * renamed into place. */
+int kites_csc_save(const char *path, uint64_t n_vertices, uint64_t n_edges,
+                   const uint64_t *R, const uint32_t *C, const uint32_t *E, int directed,
+                   const char *desc);
+/* Sizes and flags of a CSC file; desc (may be NULL) receives its description. */
+int kites_csc_info(const char *path, uint64_t *n_vertices, uint64_t *n_edges,
+                   int *has_values, int *directed, char *desc, size_t desc_len);
+/* Reads a CSC file into caller arrays sized from kites_csc_info (E may be
+ * NULL to skip the edge values). */
+int kites_csc_load(const char *path, uint64_t *R, uint32_t *C, uint32_t *E);
 
 #ifdef __cplusplus
 }  /* extern "C" */

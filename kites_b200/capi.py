@@ -38,7 +38,7 @@ EXPORTED = [
     "kites_selector_load", "kites_selector_save", "kites_graph_set_tpv",
     "kites_sssp_multi_seed", "kites_gen_rmat_union", "kites_autotune",
     "kites_graph_set_density", "kites_sssp_noalloc", "kites_graph_from_edges",
-    "kites_graph_set_batch_gather",
+    "kites_graph_set_batch_gather", "kites_csc_save", "kites_csc_info", "kites_csc_load",
 ]
 SELECTOR_FEATURES, SELECTOR_CLASSES, SELECTOR_PARAMS = 12, 4, 1628
 # Parameter layout of the selector MLP (offsets into the 1628 floats).
@@ -168,6 +168,10 @@ def load(path: str = LIB_PATH):
                                        POINTER(c_uint32)]),
         "kites_graph_from_edges": (c_int, [vp, u64, u64, vp, vp, vp, c_int, vp]),
         "kites_graph_set_batch_gather": (c_int, [vp, c_int]),
+        "kites_csc_save": (c_int, [c_char_p, u64, u64, vp, vp, vp, c_int, c_char_p]),
+        "kites_csc_info": (c_int, [c_char_p, POINTER(c_uint64), POINTER(c_uint64),
+                                   POINTER(c_int), POINTER(c_int), c_char_p, ctypes.c_size_t]),
+        "kites_csc_load": (c_int, [c_char_p, vp, vp, vp]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)
@@ -530,4 +534,36 @@ def csc_from_edges(n_vertices, src, dst, w=None):
         w = np.ascontiguousarray(w, dtype=np.uint32)
     _check(load().kites_csc_from_edges(n_vertices, m, _p(src), _p(dst), _p(w), _p(R),
                                        _p(C), _p(E)))
+    return R, C, E
+
+
+# ---------------------------------------------------------------------------
+# Binary CSC files (kites_csc_save / kites_csc_info / kites_csc_load)
+# ---------------------------------------------------------------------------
+
+def csc_save(path, R, C, E=None, directed=True, desc=""):
+    R = np.ascontiguousarray(R, dtype=np.uint64)
+    C = np.ascontiguousarray(C, dtype=np.uint32)
+    if E is not None:
+        E = np.ascontiguousarray(E, dtype=np.uint32)
+    _check(load().kites_csc_save(os.fsencode(path), R.shape[0] - 1, C.shape[0], _p(R), _p(C),
+                                 _p(E), 1 if directed else 0, desc.encode()))
+
+
+def csc_info(path):
+    """(n_vertices, n_edges, has_values, directed, desc) of a CSC file."""
+    n, m, hv, dr = c_uint64(), c_uint64(), c_int(), c_int()
+    buf = ctypes.create_string_buffer(96)
+    _check(load().kites_csc_info(os.fsencode(path), ctypes.byref(n), ctypes.byref(m),
+                                 ctypes.byref(hv), ctypes.byref(dr), buf, 96))
+    return n.value, m.value, bool(hv.value), bool(dr.value), buf.value.decode()
+
+
+def csc_load(path):
+    """(R uint64, C, E or None) of a CSC file."""
+    n, m, hv, _, _ = csc_info(path)
+    R = np.empty(n + 1, dtype=np.uint64)
+    C = np.empty(m, dtype=np.uint32)
+    E = np.empty(m, dtype=np.uint32) if hv else None
+    _check(load().kites_csc_load(os.fsencode(path), _p(R), _p(C), _p(E)))
     return R, C, E

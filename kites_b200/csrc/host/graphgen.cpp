@@ -4,7 +4,9 @@
 // destinations, each row sorted by source, ties kept in input order).
 #include <omp.h>
 #include <stdint.h>
+#include <stdio.h>
 #include <string.h>
+#include <unistd.h>
 
 #include <algorithm>
 #include <cmath>
@@ -309,5 +311,137 @@ extern "C" int kites_gen_rmat_union(uint32_t n_graphs, uint64_t seed, uint32_t v
     }
   }
   if (bad) return kites_internal::fail(KITES_ERR_INVALID, "a union member could not be generated");
+  return KITES_OK;
+}
+
+// ---- binary CSC files ------------------------------------------------------
+//
+// The prepared text format of the reference (kites/io/graph_output.cuh:23-38,
+// read back by kites/graph/graph_csr.h:112-166) holds one value per line; at
+// R-MAT scale 24 that is about 6 GB of text and minutes of parsing.  This is
+// the same CSC as raw little-endian arrays behind a 128-byte header:
+//   char     magic[8]      "KITESCSC"
+//   uint32   version       1
+//   uint32   flags         1: edge values present, 2: directed
+//   uint64   n_vertices, n_edges
+//   uint64   reserved      0
+//   char     desc[88]      NUL-padded ASCII: how the graph was made
+// then R (n_vertices + 1 uint64), C (n_edges uint32), E (n_edges uint32, if
+// flag 1).  Files are written under a temporary name and renamed, so a
+// reader never sees a partial file.
+namespace {
+
+struct csc_file_header {
+  char magic[8];
+  uint32_t version;
+  uint32_t flags;
+  uint64_t n_vertices;
+  uint64_t n_edges;
+  uint64_t reserved;
+  char desc[88];
+};
+static_assert(sizeof(csc_file_header) == 128, "CSC file header is 128 bytes");
+
+constexpr char kCscMagic[8] = {'K', 'I', 'T', 'E', 'S', 'C', 'S', 'C'};
+
+bool write_all(FILE *f, const void *p, size_t bytes) {
+  return bytes == 0 || fwrite(p, 1, bytes, f) == bytes;
+}
+
+bool read_all(FILE *f, void *p, size_t bytes) {
+  return bytes == 0 || fread(p, 1, bytes, f) == bytes;
+}
+
+int read_csc_header(const char *path, FILE **fout, csc_file_header *h) {
+  FILE *f = fopen(path, "rb");
+  if (!f) return kites_internal::fail(KITES_ERR_INVALID, "cannot open %s", path);
+  if (!read_all(f, h, sizeof(*h)) || memcmp(h->magic, kCscMagic, 8) != 0 || h->version != 1) {
+    fclose(f);
+    return kites_internal::fail(KITES_ERR_INVALID, "%s is not a version-1 CSC file", path);
+  }
+  const uint64_t want = sizeof(*h) + 8ull * (h->n_vertices + 1) +
+                        4ull * h->n_edges * ((h->flags & 1u) ? 2u : 1u);
+  if (fseeko(f, 0, SEEK_END) != 0 || (uint64_t)ftello(f) != want ||
+      fseeko(f, sizeof(*h), SEEK_SET) != 0) {
+    fclose(f);
+    return kites_internal::fail(KITES_ERR_INVALID, "%s is truncated or has trailing bytes", path);
+  }
+  *fout = f;
+  return KITES_OK;
+}
+
+}  // namespace
+
+extern "C" int kites_csc_save(const char *path, uint64_t n_vertices, uint64_t n_edges,
+                              const uint64_t *R, const uint32_t *C, const uint32_t *E,
+                              int directed, const char *desc) {
+  kites_internal::clear_error();
+  if (!path || !R || (n_edges && !C))
+    return kites_internal::fail(KITES_ERR_INVALID, "null CSC file argument");
+  if (R[0] != 0 || R[n_vertices] != n_edges)
+    return kites_internal::fail(KITES_ERR_INVALID, "R does not span 0 .. n_edges");
+  csc_file_header h;
+  memset(&h, 0, sizeof(h));
+  memcpy(h.magic, kCscMagic, 8);
+  h.version = 1;
+  h.flags = (E ? 1u : 0u) | (directed ? 2u : 0u);
+  h.n_vertices = n_vertices;
+  h.n_edges = n_edges;
+  if (desc) strncpy(h.desc, desc, sizeof(h.desc) - 1);
+  char tmp[4096];
+  if (snprintf(tmp, sizeof(tmp), "%s.tmp%ld", path, (long)getpid()) >= (int)sizeof(tmp))
+    return kites_internal::fail(KITES_ERR_INVALID, "path too long");
+  FILE *f = fopen(tmp, "wb");
+  if (!f) return kites_internal::fail(KITES_ERR_INVALID, "cannot create %s", tmp);
+  bool ok = write_all(f, &h, sizeof(h)) && write_all(f, R, 8ull * (n_vertices + 1)) &&
+            write_all(f, C, 4ull * n_edges) && (!E || write_all(f, E, 4ull * n_edges));
+  ok = (fclose(f) == 0) && ok;
+  if (!ok || rename(tmp, path) != 0) {
+    remove(tmp);
+    return kites_internal::fail(KITES_ERR_INVALID, "writing %s failed", path);
+  }
+  return KITES_OK;
+}
+
+extern "C" int kites_csc_info(const char *path, uint64_t *n_vertices, uint64_t *n_edges,
+                              int *has_values, int *directed, char *desc, size_t desc_len) {
+  kites_internal::clear_error();
+  if (!path) return kites_internal::fail(KITES_ERR_INVALID, "null path");
+  FILE *f = nullptr;
+  csc_file_header h;
+  int st = read_csc_header(path, &f, &h);
+  if (st != KITES_OK) return st;
+  fclose(f);
+  if (n_vertices) *n_vertices = h.n_vertices;
+  if (n_edges) *n_edges = h.n_edges;
+  if (has_values) *has_values = (h.flags & 1u) ? 1 : 0;
+  if (directed) *directed = (h.flags & 2u) ? 1 : 0;
+  if (desc && desc_len) {
+    const size_t k = std::min(desc_len - 1, strnlen(h.desc, sizeof(h.desc)));
+    memcpy(desc, h.desc, k);
+    desc[k] = '\0';
+  }
+  return KITES_OK;
+}
+
+extern "C" int kites_csc_load(const char *path, uint64_t *R, uint32_t *C, uint32_t *E) {
+  kites_internal::clear_error();
+  if (!path || !R) return kites_internal::fail(KITES_ERR_INVALID, "null CSC file argument");
+  FILE *f = nullptr;
+  csc_file_header h;
+  int st = read_csc_header(path, &f, &h);
+  if (st != KITES_OK) return st;
+  if (h.n_edges && !C) {
+    fclose(f);
+    return kites_internal::fail(KITES_ERR_INVALID, "null C for a graph with edges");
+  }
+  bool ok = read_all(f, R, 8ull * (h.n_vertices + 1)) && read_all(f, C, 4ull * h.n_edges);
+  if (ok && (h.flags & 1u)) {
+    if (E) ok = read_all(f, E, 4ull * h.n_edges);
+  }
+  fclose(f);
+  if (!ok) return kites_internal::fail(KITES_ERR_INVALID, "reading %s failed", path);
+  if (R[0] != 0 || R[h.n_vertices] != h.n_edges)
+    return kites_internal::fail(KITES_ERR_INVALID, "%s: R does not span 0 .. n_edges", path);
   return KITES_OK;
 }

@@ -43,7 +43,7 @@ def build_oracle_lib() -> str:
     os.makedirs(os.path.dirname(LIB_PATH), exist_ok=True)
     if (not os.path.exists(LIB_PATH)
             or os.path.getmtime(LIB_PATH) < os.path.getmtime(src)):
-        subprocess.check_call(["gcc", "-O2", "-fPIC", "-shared", "-std=c11",
+        subprocess.check_call(["gcc", "-O2", "-fPIC", "-shared", "-std=c11", "-fopenmp",
                                "-o", LIB_PATH, src])
     return LIB_PATH
 
@@ -68,6 +68,12 @@ def lib():
         _lib.kor_jacobi_fixed_point.restype = u64
         _lib.kor_jacobi_fixed_point.argtypes = [ctypes.c_int, u64, p, p, p,
                                                 p, p]
+        _lib.kor_gen_rmat.restype = ctypes.c_int
+        _lib.kor_gen_rmat.argtypes = [ctypes.c_uint32, u64, u64, ctypes.c_double,
+                                      ctypes.c_double, ctypes.c_double, u64,
+                                      ctypes.c_uint32, ctypes.c_uint32, p, p, p]
+        _lib.kor_csc_from_edges.restype = ctypes.c_int
+        _lib.kor_csc_from_edges.argtypes = [u64, u64, p, p, p, p, p, p]
     return _lib
 
 
@@ -305,6 +311,36 @@ def read_edge_list(path):
 # --------------------------------------------------------------------------
 # Fixed points
 # --------------------------------------------------------------------------
+
+def gen_rmat(scale, n_edges, a=0.57, b=0.19, c=0.19, seed=1, w_lo=1, w_hi=255,
+             n_vertices=0):
+    """The benchmark's R-MAT edge list from the oracle's own restatement of
+    the generator rule (kor_gen_rmat): same (src, dst, w) as the product's
+    generator for the same arguments."""
+    src = np.empty(n_edges, dtype=np.uint32)
+    dst = np.empty(n_edges, dtype=np.uint32)
+    w = np.empty(n_edges, dtype=np.uint32)
+    if lib().kor_gen_rmat(scale, n_vertices, n_edges, a, b, c, seed, w_lo, w_hi, _ptr(src),
+                          _ptr(dst), _ptr(w)) != 0:
+        raise MemoryError("kor_gen_rmat failed")
+    return src, dst, w
+
+
+def csc_from_edges(n_vertices, src, dst, w=None):
+    """CSC (rows = destinations, sources ascending, ties in input order) of
+    an edge list, by the oracle's own builder (kor_csc_from_edges)."""
+    src = np.ascontiguousarray(src, dtype=np.uint32)
+    dst = np.ascontiguousarray(dst, dtype=np.uint32)
+    m = src.shape[0]
+    R = np.empty(n_vertices + 1, dtype=np.uint64)
+    C = np.empty(m, dtype=np.uint32)
+    E = np.empty(m, dtype=np.uint32) if w is not None else None
+    w = None if w is None else np.ascontiguousarray(w, dtype=np.uint32)
+    if lib().kor_csc_from_edges(n_vertices, m, _ptr(src), _ptr(dst), _ptr(w), _ptr(R),
+                                _ptr(C), _ptr(E)) != 0:
+        raise ValueError("kor_csc_from_edges failed (bad endpoint or out of memory)")
+    return R, C, E
+
 
 def sanity_check(hg_or_R, C=None, E=None, V=None, op=OP_SSSP_SAT):
     """Gauss-Seidel fixed point (sanity_check.cuh:22-47). Returns (V, sweeps)."""

@@ -300,3 +300,77 @@ extern "C" double ref_sanity_check_csc(int op, uint64_t n, uint64_t m,
     return -1.0;
   }
 }
+
+// ---- many sources on all host threads (bench.py's reference arm) ----------
+// SSSP (saturating add, the engine's KITES_OP_SSSP) from each of `n_sources`
+// sources over one graph, each by the reference's own sanity_check loop
+// (sanity_check.cuh:13-59), which is single-threaded: `threads` host threads
+// take sources one at a time and run their loops side by side, sharing one
+// copy of R, C and E in the reference's host buffers.  For source i,
+// reached_edges[i] = the sum of out_degree over the vertices it reaches and
+// secs_each[i] the wall seconds of its loop; dist_out (n x n_sources, column
+// i at dist_out + i * n) may be NULL.  Returns the wall seconds from the
+// first loop's start to the last one's end, or a negative value on error.
+#include <atomic>
+#include <thread>
+
+extern "C" double ref_sssp_sources(uint64_t n, uint64_t m, const uint32_t *R,
+                                   const uint32_t *C, const uint32_t *E,
+                                   const uint32_t *sources, uint32_t n_sources,
+                                   uint32_t threads, const uint64_t *out_degree,
+                                   uint64_t *reached_edges, double *secs_each,
+                                   uint32_t *dist_out) {
+  using vT = unsigned;
+  using eT = unsigned;
+  try {
+    if (m >= 0x80000000ull) return -2.0;  // the loop masks bit 31 of offsets
+    kites::host_pinned_buffer<unsigned> Rb(n + 1), Cb(m ? m : 1);
+    kites::host_pinned_buffer<eT> Eb(m ? m : 1);
+    std::memcpy(Rb.get_ptr(), R, (n + 1) * sizeof(unsigned));
+    if (m) std::memcpy(Cb.get_ptr(), C, m * sizeof(unsigned));
+    if (m && E) std::memcpy(Eb.get_ptr(), E, m * sizeof(eT));
+    std::atomic<uint32_t> next{0};
+    std::atomic<bool> failed{false};
+    auto worker = [&]() {
+      try {
+        kites::host_pinned_buffer<vT> V(n), Vcopy(n);
+        for (uint32_t i; (i = next.fetch_add(1)) < n_sources;) {
+          const uint32_t s = sources[i];
+          for (uint64_t v = 0; v < n; ++v) V[v] = 0xFFFFFFFFu;
+          V[s] = 0u;
+          std::memcpy(Vcopy.get_ptr(), V.get_ptr(), n * sizeof(vT));
+          auto initF = [](volatile vT &l, vT &g) { l = g; };
+          auto redF = [](volatile vT &l, volatile vT &r) { if (l > r) l = r; };
+          auto updF = [](volatile vT &nv, vT o) { return nv < o; };
+          auto comp = [](volatile vT &p, vT sv, eT *w) {
+            vT t = sv + *w;
+            p = (t < sv) ? 0xFFFFFFFFu : t;
+          };
+          auto t0 = std::chrono::steady_clock::now();
+          kites::sanity_check(n, V, Rb, Cb, Eb, Vcopy, initF, comp, redF, updF);
+          auto t1 = std::chrono::steady_clock::now();
+          if (secs_each) secs_each[i] = std::chrono::duration<double>(t1 - t0).count();
+          if (reached_edges && out_degree) {
+            uint64_t r = 0;
+            for (uint64_t v = 0; v < n; ++v)
+              if (V[v] != 0xFFFFFFFFu) r += out_degree[v];
+            reached_edges[i] = r;
+          }
+          if (dist_out) std::memcpy(dist_out + (uint64_t)i * n, V.get_ptr(), n * sizeof(vT));
+        }
+      } catch (...) {
+        failed = true;
+      }
+    };
+    const uint32_t nt = std::max<uint32_t>(1, std::min(threads, n_sources));
+    auto t0 = std::chrono::steady_clock::now();
+    std::vector<std::thread> pool;
+    for (uint32_t t = 0; t < nt; ++t) pool.emplace_back(worker);
+    for (auto &th : pool) th.join();
+    auto t1 = std::chrono::steady_clock::now();
+    if (failed) return -1.0;
+    return std::chrono::duration<double>(t1 - t0).count();
+  } catch (...) {
+    return -1.0;
+  }
+}

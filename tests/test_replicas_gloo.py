@@ -66,16 +66,19 @@ def test_reductions_and_disjoint_sources_over_two_gloo_ranks(tmp_path):
 
 @pytest.mark.skipif(not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libref_harness.so")),
                     reason="reference harness not built")
-def test_reference_arm_under_torchrun_prints_once():
+def test_reference_arm_under_torchrun_prints_once(tmp_path):
     port = free_port()
     cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
            "--master-addr", "127.0.0.1", "--master-port", str(port), "bench.py", "--impl",
-           "reference", "--gpus", "2", "--steps", "1", "--warmup", "1",
-           "--ref-sample-scale", "12"]
-    out = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, timeout=300)
+           "reference", "--gpus", "2", "--steps", "2", "--warmup", "1", "--scale", "12"]
+    env = dict(os.environ, KITES_GRAPH_CACHE=str(tmp_path))
+    out = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, timeout=300, env=env)
     assert out.returncode == 0, out.stderr[-2000:]
     lines = [ln for ln in out.stdout.splitlines() if ln.startswith("{")]
     assert len(lines) == 1
     rec = json.loads(lines[0])
     assert rec["impl"] == "reference" and rec["value"] > 0 and rec["n_gpus"] == 2
     assert rec["e2e"]["h2d_bytes_per_step"] == 0
+    assert rec["config"]["workload"] == "sssp_rmat_scale12" and rec["cpu_baseline"]["cores"] >= 1
+    # The reference process wrote the graph through the oracle alone.
+    assert os.listdir(tmp_path) == ["rmat12_ef16_seed1.csc"]
