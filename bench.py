@@ -70,7 +70,8 @@ def parse():
                     help="batch: --batch sources per pass over the edges (headline); "
                          "single: one source at a time through kites_sssp")
     ap.add_argument("--strategy", default="plain", choices=sorted(STRATEGIES),
-                    help="per-iteration strategy of --mode single (batch runs plain)")
+                    help="per-iteration strategy: auto = the learned selector; batch mode "
+                         "takes plain, auto, push, pull_all and pull_changed")
     ap.add_argument("--batch-gather", default="loads", choices=["loads", "tma"],
                     help="how the batched pull fetches source rows: register loads or "
                          "TMA tile::gather4 copies")
@@ -401,8 +402,9 @@ def run_ours(args):
     if args.mode == "batch" and args.sources % K:
         raise SystemExit("--sources must be a multiple of --batch")
     groups = [srcs[i:i + K] for i in range(0, len(srcs), K)]
-    if args.mode == "batch" and args.strategy != "plain":
-        raise SystemExit("--mode batch runs the plain strategy")
+    if args.mode == "batch" and args.strategy not in ("plain", "auto", "push", "pull_all",
+                                                      "pull_changed"):
+        raise SystemExit(f"--mode batch does not take --strategy {args.strategy}")
     tuned = None
     if not args.no_autotune:
         r = g.autotune(srcs[:8], batch=K if args.mode == "batch" else 16)
@@ -410,7 +412,7 @@ def run_ours(args):
                  "dense_edges": int(r.dense_edges), "dense_rows": int(r.dense_rows),
                  "tpv_strategy": int(r.tpv_strategy), "trials": int(r.trials)}
     loop = 0 if args.host_loop else 1
-    bopts = capi.default_opts(device_loop=loop)
+    bopts = capi.default_opts(device_loop=loop, strategy=STRATEGIES[args.strategy])
     sopts = capi.default_opts(device_loop=loop, strategy=STRATEGIES[args.strategy])
     lib = capi.load()
 
@@ -473,6 +475,29 @@ def run_ours(args):
         pms = reduce_over_ranks(p0.elapsed_time(p1), world, device, "MAX")
         plain = {"value": reduce_over_ranks(units_per_step, world, device, "SUM") /
                  (pms * 1e-3) / 1e9, "unit": UNIT, "ms_per_step": pms}
+
+    # The fixed batched pull (strategy plain) on the same batches, beside a
+    # batched run with another strategy.
+    batched_plain = None
+    if args.mode == "batch" and args.strategy != "plain":
+        fixed = capi.default_opts(device_loop=loop)
+        for grp in groups:
+            capi._check(lib.kites_sssp_batch(eng._h, g._h, capi.OP_SSSP, capi._p(grp), K, None,
+                                             ctypes.byref(fixed), None))
+        barrier(world)
+        torch.cuda.synchronize()
+        q0 = torch.cuda.Event(enable_timing=True)
+        q1 = torch.cuda.Event(enable_timing=True)
+        q0.record(stream)
+        for _ in range(args.steps):
+            for grp in groups:
+                capi._check(lib.kites_sssp_batch(eng._h, g._h, capi.OP_SSSP, capi._p(grp), K,
+                                                 None, ctypes.byref(fixed), None))
+        q1.record(stream)
+        torch.cuda.synchronize()
+        qms = reduce_over_ranks(q0.elapsed_time(q1), world, device, "MAX")
+        batched_plain = {"value": total_units / (qms * 1e-3) / 1e9, "unit": UNIT,
+                         "ms_per_step": qms / args.steps}
 
     # Rooflines of the dominant kernels, timed live with CUDA events around
     # every launch (host loop): k_pull_batch for the headline, k_pull_chunked
@@ -598,6 +623,9 @@ def run_ours(args):
             "gpu_launches": int(launches),
             "plain": plain,
             "speedup_vs_plain": (value / plain["value"]) if plain else None,
+            "batched_plain": batched_plain,
+            "speedup_vs_batched_plain": (value / batched_plain["value"]) if batched_plain
+            else None,
             "roofline": ({"bound": "hbm", "achieved": b_ach, "peak": peak, "unit": "GB/s",
                           "frac": b_ach / peak, "traffic": traffic,
                           "kernel": f"k_pull_batch<SSSP,K={K}>",

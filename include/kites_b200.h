@@ -20,7 +20,7 @@
 extern "C" {
 #endif
 
-#define KITES_B200_ABI_VERSION 1
+#define KITES_B200_ABI_VERSION 2
 
 typedef enum kites_status {
   KITES_OK = 0,
@@ -52,7 +52,10 @@ typedef enum kites_op {
  * bitmap frontier (kites/device/kernels_single_device.cuh:18-426 re-designed);
  * AUTO lets the learned selector pick per iteration, falling back to PLAIN
  * when the predicted gain is under the margin.  The others force one
- * strategy for every iteration (used to record training timings). */
+ * strategy for every iteration (used to record training timings).
+ * Batched runs (kites_sssp_batch) take PLAIN, AUTO, PUSH, PULL_ALL and
+ * PULL_CHANGED; there PUSH, PULL_ALL and PULL_CHANGED move only the 32-byte
+ * sectors of each source row that changed in the previous iteration. */
 typedef enum kites_strategy {
   KITES_STRATEGY_PLAIN = 0,
   KITES_STRATEGY_AUTO = 1,
@@ -62,7 +65,9 @@ typedef enum kites_strategy {
   KITES_STRATEGY_TPV4 = 5,      /* pull, 4 threads per active vertex         */
   KITES_STRATEGY_TPV8 = 6,      /* pull, 8 threads per active vertex         */
   KITES_STRATEGY_TPV32 = 7,     /* pull, one warp per active vertex          */
-  KITES_STRATEGY_COUNT = 8
+  KITES_STRATEGY_PULL_CHANGED = 8,  /* pull over the frontier, reading only
+                                       in-neighbours that changed last time  */
+  KITES_STRATEGY_COUNT = 9
 } kites_strategy;
 
 typedef struct kites_engine kites_engine;
@@ -190,7 +195,7 @@ int kites_graph_upload(kites_engine *eng, const kites_csc_view *view,
  * (kites/graph/graph_raw.h:57-190) sorts on the host: rows keyed by
  * destination, each row's sources ascending, parallel edges kept in input
  * order.  src, dst, weights (NULL: unweighted): n_edges uint32 each, host or
- * device memory; n_edges < 2^31.  directed = 0 expects both directions of
+ * device memory; n_edges < 2^32.  directed = 0 expects both directions of
  * every undirected edge in the list; vpg 1, vertex values 4 bytes, no
  * initial values or frontier (set them with kites_graph_set_*). */
 int kites_graph_from_edges(kites_engine *eng, uint64_t n_vertices, uint64_t n_edges,
@@ -222,7 +227,10 @@ int kites_sssp(kites_engine *eng, kites_graph *g, int op, uint32_t source,
                kites_run_stats *stats);
 
 /* Batched multi-source SSSP/BFS: K sources at once, distances in a
- * V x K vertex-major array (dist_out[v*K + k]); K is 16, 32, 64, 128 or 256. */
+ * V x K vertex-major array (dist_out[v*K + k]); K is 16, 32, 64, 128 or 256.
+ * opts->strategy: PLAIN (the K-wide pull every iteration), or -- for the
+ * saturating SSSP and BFS on graphs with vertex_per_group 1 -- AUTO (the
+ * batched learned selector), PUSH, PULL_ALL or PULL_CHANGED. */
 int kites_sssp_batch(kites_engine *eng, kites_graph *g, int op,
                      const uint32_t *sources, uint32_t k, uint32_t *dist_out,
                      const kites_run_opts *opts, kites_run_stats *stats);
@@ -288,6 +296,21 @@ int kites_selector_train(kites_engine *eng, const float *features, const float *
                          uint64_t seed, float *params_out, float *final_loss);
 int kites_selector_load(kites_engine *eng, const float *params, uint32_t n_params);
 int kites_selector_save(kites_engine *eng, float *params, uint32_t n_params);
+/* The same fit, returning the parameters without loading them anywhere. */
+int kites_selector_fit(kites_engine *eng, const float *features, const float *times_ms,
+                       uint32_t n_records, uint32_t epochs, float learning_rate, uint64_t seed,
+                       float *params_out, float *final_loss);
+/* The batched loop's selector (kites_sssp_batch with KITES_STRATEGY_AUTO):
+ * the same MLP and features over the batch's changed set, with its own
+ * weights; classes PLAIN, PUSH, PULL_ALL, PULL_CHANGED.  Training data: a
+ * K-source batched run where every iteration times each class from the
+ * same state (D, changed set and changed sectors restored after each) and
+ * then advances with PLAIN; times_ms: capacity x 4 in class order. */
+int kites_selector_record_batch(kites_engine *eng, kites_graph *g, int op,
+                                const uint32_t *sources, uint32_t k, float *features,
+                                float *times_ms, uint32_t capacity, uint32_t *n_records);
+int kites_selector_load_batch(kites_engine *eng, const float *params, uint32_t n_params);
+int kites_selector_save_batch(kites_engine *eng, float *params, uint32_t n_params);
 /* Threads-per-vertex width of the selector's TPV class for this graph
  * (KITES_STRATEGY_TPV1/4/8/32). */
 int kites_graph_set_tpv(kites_graph *g, int strategy);

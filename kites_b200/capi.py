@@ -21,8 +21,8 @@ LIB_PATH = os.path.join(HERE, "libkites_b200.so")
 OK, ERR_INVALID, ERR_OOM, ERR_CUDA, ERR_TIMEOUT, ERR_UNSUPPORTED, ERR_NO_DEVICE = range(7)
 OP_SSSP, OP_SSSP_WRAP, OP_BFS, OP_CC, OP_PAGERANK = range(5)
 (STRATEGY_PLAIN, STRATEGY_AUTO, STRATEGY_PUSH, STRATEGY_PULL_ALL, STRATEGY_TPV1,
- STRATEGY_TPV4, STRATEGY_TPV8, STRATEGY_TPV32) = range(8)
-STRATEGY_COUNT = 8
+ STRATEGY_TPV4, STRATEGY_TPV8, STRATEGY_TPV32, STRATEGY_PULL_CHANGED) = range(9)
+STRATEGY_COUNT = 9
 MAX_RECORDED_ITERS = 4096
 INF = 0xFFFFFFFF
 
@@ -39,7 +39,11 @@ EXPORTED = [
     "kites_sssp_multi_seed", "kites_gen_rmat_union", "kites_autotune",
     "kites_graph_set_density", "kites_sssp_noalloc", "kites_graph_from_edges",
     "kites_graph_set_batch_gather", "kites_csc_save", "kites_csc_info", "kites_csc_load",
+    "kites_selector_fit", "kites_selector_record_batch", "kites_selector_load_batch",
+    "kites_selector_save_batch",
 ]
+# Selector classes of the batched loop (kites_sssp_batch with AUTO).
+BATCH_CLASS_STRATEGY = [STRATEGY_PLAIN, STRATEGY_PUSH, STRATEGY_PULL_ALL, STRATEGY_PULL_CHANGED]
 SELECTOR_FEATURES, SELECTOR_CLASSES, SELECTOR_PARAMS = 12, 4, 1628
 # Parameter layout of the selector MLP (offsets into the 1628 floats).
 SEL_OFF = {"mean": 0, "std": 12, "W1": 24, "b1": 408, "W2": 440, "b2": 1464, "W3": 1496,
@@ -172,6 +176,12 @@ def load(path: str = LIB_PATH):
         "kites_csc_info": (c_int, [c_char_p, POINTER(c_uint64), POINTER(c_uint64),
                                    POINTER(c_int), POINTER(c_int), c_char_p, ctypes.c_size_t]),
         "kites_csc_load": (c_int, [c_char_p, vp, vp, vp]),
+        "kites_selector_fit": (c_int, [vp, vp, vp, u32, u32, c_float, u64, vp,
+                                       POINTER(c_float)]),
+        "kites_selector_record_batch": (c_int, [vp, vp, c_int, vp, u32, vp, vp, u32,
+                                                POINTER(c_uint32)]),
+        "kites_selector_load_batch": (c_int, [vp, vp, u32]),
+        "kites_selector_save_batch": (c_int, [vp, vp, u32]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)
@@ -268,6 +278,25 @@ class Engine:
     def selector_save(self):
         P = np.empty(SELECTOR_PARAMS, dtype=np.float32)
         _check(load().kites_selector_save(self._h, _p(P), SELECTOR_PARAMS))
+        return P
+
+    def selector_fit(self, features, times_ms, epochs=2000, lr=3e-3, seed=1):
+        """Fits the MLP to recorded timings; returns (params, loss), loads nothing."""
+        X = np.ascontiguousarray(features, dtype=np.float32)
+        T = np.ascontiguousarray(times_ms, dtype=np.float32)
+        params = np.empty(SELECTOR_PARAMS, dtype=np.float32)
+        loss = c_float()
+        _check(load().kites_selector_fit(self._h, _p(X), _p(T), X.shape[0], epochs, lr, seed,
+                                         _p(params), ctypes.byref(loss)))
+        return params, loss.value
+
+    def selector_load_batch(self, params):
+        P = np.ascontiguousarray(params, dtype=np.float32)
+        _check(load().kites_selector_load_batch(self._h, _p(P), P.shape[0]))
+
+    def selector_save_batch(self):
+        P = np.empty(SELECTOR_PARAMS, dtype=np.float32)
+        _check(load().kites_selector_save_batch(self._h, _p(P), SELECTOR_PARAMS))
         return P
 
 
@@ -436,6 +465,18 @@ class Graph:
         n = c_uint32()
         _check(load().kites_selector_record(self.engine._h, self._h, op, source, _p(X), _p(T),
                                             capacity, ctypes.byref(n)))
+        return X[: n.value], T[: n.value]
+
+    def selector_record_batch(self, sources, op=OP_SSSP, capacity=512):
+        """Per iteration of a batched run: 12 features and the time (ms) of
+        each batched class (PLAIN, PUSH, PULL_ALL, PULL_CHANGED)."""
+        src = np.ascontiguousarray(sources, dtype=np.uint32)
+        X = np.zeros((capacity, SELECTOR_FEATURES), dtype=np.float32)
+        T = np.zeros((capacity, SELECTOR_CLASSES), dtype=np.float32)
+        n = c_uint32()
+        _check(load().kites_selector_record_batch(self.engine._h, self._h, op, _p(src),
+                                                  src.shape[0], _p(X), _p(T), capacity,
+                                                  ctypes.byref(n)))
         return X[: n.value], T[: n.value]
 
     def set_batch_gather(self, mode):

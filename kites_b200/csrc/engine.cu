@@ -43,6 +43,16 @@ static const float kDefaultSelector[] = {
 static_assert(sizeof(kDefaultSelector) == kParams * sizeof(float),
               "selector_default.inc must hold the 1628 selector parameters");
 #endif
+// The batched loop's selector (classes PLAIN, PUSH, PULL_ALL, PULL_CHANGED),
+// written by `python -m kites_b200.train_selector --batch --inc ...`.
+#if __has_include("selector_batch_default.inc")
+#define KITES_HAVE_DEFAULT_BATCH_SELECTOR 1
+static const float kDefaultBatchSelector[] = {
+#include "selector_batch_default.inc"
+};
+static_assert(sizeof(kDefaultBatchSelector) == kParams * sizeof(float),
+              "selector_batch_default.inc must hold the 1628 selector parameters");
+#endif
 
 int dev_alloc(kites_engine *eng, void **p, size_t bytes) {
   *p = nullptr;
@@ -191,8 +201,9 @@ int build_out_csr(kites_graph *g) {
   KITES_TRY(graph_alloc(g, &p, (n + 1) * sizeof(uint32_t)));
   g->out_deg = (uint32_t *)p;
   KITES_CUDA_TRY(cudaMemsetAsync(g->out_deg, 0, (n + 1) * sizeof(uint32_t), s));
-  if (m > 0x7FFFFFFFull)
-    return fail(KITES_ERR_UNSUPPORTED, "out-CSR build supports < 2^31 edges");
+  // The transposition sorts 32-bit edge ids (item counts are 64-bit).
+  if (m > 0xFFFFFFFFull)
+    return fail(KITES_ERR_UNSUPPORTED, "out-CSR build supports < 2^32 edges");
   if (m) {
     k_count_u32<<<grid_for(m), 256, 0, s>>>(g->C, m, g->out_deg);
     KITES_CUDA_TRY(cudaGetLastError());
@@ -204,11 +215,11 @@ int build_out_csr(kites_graph *g) {
   k_widen_offsets<OffT><<<grid_for(n + 1), 256, 0, s>>>(g->out_deg, n + 1, deg_wide);
   size_t temp_bytes = 0;
   KITES_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, temp_bytes, deg_wide,
-                                               (OffT *)g->outR, (int)(n + 1), s));
+                                               (OffT *)g->outR, (uint64_t)(n + 1), s));
   void *temp;
   KITES_TRY(dev_alloc(eng, &temp, temp_bytes));
   KITES_CUDA_TRY(cub::DeviceScan::ExclusiveSum(temp, temp_bytes, deg_wide,
-                                               (OffT *)g->outR, (int)(n + 1), s));
+                                               (OffT *)g->outR, (uint64_t)(n + 1), s));
   KITES_CUDA_TRY(cudaFreeAsync(temp, s));
   KITES_CUDA_TRY(cudaFreeAsync(deg_wide, s));
   if (m == 0) return KITES_OK;
@@ -225,10 +236,10 @@ int build_out_csr(kites_graph *g) {
   while (end_bit < 32 && (1ull << end_bit) < n) ++end_bit;
   temp_bytes = 0;
   KITES_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, temp_bytes, g->C, keys_out,
-                                                 idx_in, idx_out, (int)m, 0, end_bit, s));
+                                                 idx_in, idx_out, (uint64_t)m, 0, end_bit, s));
   KITES_TRY(dev_alloc(eng, &temp, temp_bytes));
   KITES_CUDA_TRY(cub::DeviceRadixSort::SortPairs(temp, temp_bytes, g->C, keys_out,
-                                                 idx_in, idx_out, (int)m, 0, end_bit, s));
+                                                 idx_in, idx_out, (uint64_t)m, 0, end_bit, s));
   k_gather_out<OffT><<<grid_for(m), 256, 0, s>>>(
       idx_out, row, g->esize == 4 ? (const uint32_t *)g->E : nullptr, m, g->outC, g->outE);
   KITES_CUDA_TRY(cudaGetLastError());
@@ -777,6 +788,14 @@ int launch_strategy(kites_graph *g, const flex_state &f, int strategy, int parit
       launch_sweep<OP, OffT, kAllRows>(g, nullptr, nullptr, Unext, 0u, 0u);
       break;
     }
+    case KITES_STRATEGY_PULL_CHANGED: {
+      // The frontier's rows fold only in-edges whose source is in U.
+      expand();
+      pull_args<OffT> pa{gin, (const uint32_t *)g->E, (uint32_t *)g->V, f.A, Unext, 0, g->ctr,
+                         Ucur, 0u, 0u, 0ull, 0ull};
+      k_pull_all<OP, OffT><<<g->pull_grid, kBlock, 0, s>>>(pa);
+      break;
+    }
     case KITES_STRATEGY_TPV1:
     case KITES_STRATEGY_TPV4:
     case KITES_STRATEGY_TPV8:
@@ -894,10 +913,11 @@ int prepare_select(kites_graph *g) {
 
 template <typename OffT>
 int launch_select(kites_graph *g, const uint32_t *U, float margin, float *feat_out,
-                  uint32_t feat_cap, cudaGraphConditionalHandle h, int hh, uint64_t *launches) {
+                  uint32_t feat_cap, cudaGraphConditionalHandle h, int hh, uint64_t *launches,
+                  const float *params = nullptr) {
   select_args<OffT> a{U, g->nwords, g->out_deg, (const OffT *)g->R, g->n, g->m, g->ctr,
-                      (select_acc *)g->sacc, g->eng->sel_params, logf(1.f + margin), feat_out,
-                      feat_cap, h, hh};
+                      (select_acc *)g->sacc, params ? params : g->eng->sel_params,
+                      logf(1.f + margin), feat_out, feat_cap, h, hh};
   k_select<OffT><<<grid_for(g->nwords, 256, (unsigned)g->eng->sm_count * 4), 256, 0,
                    g->eng->stream>>>(a);
   k_record_sel<<<1, 1, 0, g->eng->stream>>>(g->ctr, g->rec_sel, KITES_MAX_RECORDED_ITERS);
@@ -1397,6 +1417,480 @@ int dispatch_batch(kites_graph *g, int op, const uint32_t *src, uint32_t k, uint
   }
 }
 
+// ---- batched strategies (learned + batched) ---------------------------------
+//
+// The batched loop with one strategy per iteration.  Its state between
+// iterations is the changed set U (vertex bits) and, per vertex, the
+// sectors of its K-wide row that changed (M); every strategy turns
+// (U, M) into the next (U', M'):
+//   PLAIN         activation of U into the frontier A, then the K-wide pull
+//                 over A with whole source rows (k_pull_batch);
+//   PULL_CHANGED  the same frontier, gathering only the changed sectors of
+//                 each source (k_pull_batch<masked>);
+//   PULL_ALL      every row, changed sectors only, no activation pass;
+//   PUSH          the out-edges of U's rows relax the changed sectors of
+//                 their targets with atomicMin (k_push_batch).
+// AUTO lets the selector pick per iteration (k_select with the batched
+// weights, then a switch node), PLAIN being the fallback class.
+
+struct batch_flex {
+  uint32_t *D;
+  uint32_t *A;          // frontier scratch
+  uint32_t *U[2];       // changed sets by parity
+  uint32_t *M[2];       // changed sectors by parity (n words each)
+  uint64_t nwords;
+  const void *actR;
+  const uint32_t *actC;
+  const uint32_t *act_chunks;
+  uint64_t act_nchunks, act_rows, act_edges;
+  const void *outR;     // push: out-CSR and its chunk table
+  const uint32_t *out_chunks;
+  uint64_t out_nchunks;
+  int pull_grid, mpull_grid, push_grid;
+};
+
+// Selector class -> batched strategy.
+int batch_class_strategy(uint32_t cls) {
+  switch (cls) {
+    case 1: return KITES_STRATEGY_PUSH;
+    case 2: return KITES_STRATEGY_PULL_ALL;
+    case 3: return KITES_STRATEGY_PULL_CHANGED;
+    default: return KITES_STRATEGY_PLAIN;
+  }
+}
+
+template <typename OffT>
+int prepare_batch_flex(kites_graph *g, uint32_t K, batch_flex *f) {
+  if (g->vpg != 1)
+    return fail(KITES_ERR_UNSUPPORTED, "batched strategies need vertex_per_group 1");
+  batch_state b{};
+  const uint32_t items = g->batch_items_req ? g->batch_items_req : 256u;
+  KITES_TRY(prepare_batch<OffT>(g, K, items, &b));
+  void *p;
+  if (!g->bmask) {
+    KITES_TRY(graph_alloc(g, &p, 2 * g->n * 4));
+    g->bmask = (uint32_t *)p;
+  }
+  // Push walks the weighted out-CSR; for directed graphs with vpg 1 the
+  // activation adjacency is that out-CSR and its chunk table is shared.
+  const uint32_t *oc = nullptr;
+  uint64_t onc = 0;
+  if (g->dirR == g->outR) {
+    oc = g->chunk_dir;
+    onc = g->nchunks_dir;
+  } else {
+    if (!g->chunk_out)
+      KITES_TRY(build_chunk_table<OffT>(g, (const OffT *)g->outR, g->n, g->m, &g->chunk_out,
+                                        &g->nchunks_out));
+    oc = g->chunk_out;
+    onc = g->nchunks_out;
+  }
+  f->D = b.D;
+  f->nwords = b.nwords;
+  f->A = b.bits;
+  f->U[0] = b.bits + b.nwords;
+  f->U[1] = b.bits + 3 * b.nwords;
+  f->M[0] = g->bmask;
+  f->M[1] = g->bmask + g->n;
+  f->actR = b.actR;
+  f->actC = b.actC;
+  f->act_chunks = b.act_chunks;
+  f->act_nchunks = b.act_nchunks;
+  f->act_rows = b.act_rows;
+  f->act_edges = b.act_edges;
+  f->outR = g->outR;
+  f->out_chunks = oc;
+  f->out_nchunks = onc;
+  return KITES_OK;
+}
+
+template <int OP, typename OffT, int K>
+int size_batch_flex_grids(kites_graph *g, batch_flex *f) {
+  const int sms = g->eng->sm_count;
+  auto grid = [&](auto kernel, uint64_t chunks, int *out) -> int {
+    int per_sm = 0;
+    KITES_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kBlock, 0));
+    const uint64_t cap = (uint64_t)std::max(per_sm, 1) * sms;
+    const uint64_t want = (chunks + kWarpsPerBlock - 1) / kWarpsPerBlock;
+    *out = (int)std::max<uint64_t>(1, std::min(want, cap));
+    return KITES_OK;
+  };
+  KITES_TRY(grid(k_pull_batch<OP, OffT, K, false>, g->nchunks_batch, &f->pull_grid));
+  KITES_TRY(grid(k_pull_batch<OP, OffT, K, true>, g->nchunks_batch, &f->mpull_grid));
+  KITES_TRY(grid(k_push_batch<OP, OffT, K>, f->out_nchunks, &f->push_grid));
+  return KITES_OK;
+}
+
+// Enqueues one iteration's strategy: (U[parity], M[parity]) -> (U[parity^1],
+// M[parity^1]).
+template <int OP, typename OffT, int K>
+int launch_batch_strategy(kites_graph *g, const batch_flex &f, int strategy, int parity,
+                          uint64_t *launches) {
+  cudaStream_t s = g->eng->stream;
+  uint32_t *Uc = f.U[parity], *Un = f.U[parity ^ 1];
+  uint32_t *Mc = f.M[parity], *Mn = f.M[parity ^ 1];
+  chunk_geom<OffT> gb{(const OffT *)g->R, g->C, g->chunk_batch, g->nchunks_batch,
+                      g->n, g->n + g->m, g->batch_chunk_items};
+  switch (strategy) {
+    case KITES_STRATEGY_PLAIN:
+    case KITES_STRATEGY_PULL_CHANGED: {
+      // U was marked by the previous iteration: its count is last_changed.
+      launch_expand<OffT>(g, f.actR, f.actC, f.act_chunks, f.act_nchunks, true, f.act_rows,
+                          f.act_edges, Uc, f.A, 0u, launches);
+      pull_batch_args<OffT> pa{gb, (const uint32_t *)g->E, f.D, f.A, Un, g->ctr, Mc, Mn};
+      if (strategy == KITES_STRATEGY_PLAIN)
+        k_pull_batch<OP, OffT, K, false><<<f.pull_grid, kBlock, 0, s>>>(pa);
+      else
+        k_pull_batch<OP, OffT, K, true><<<f.mpull_grid, kBlock, 0, s>>>(pa);
+      break;
+    }
+    case KITES_STRATEGY_PULL_ALL: {
+      pull_batch_args<OffT> pa{gb, (const uint32_t *)g->E, f.D, nullptr, Un, g->ctr, Mc, Mn};
+      k_pull_batch<OP, OffT, K, true><<<f.mpull_grid, kBlock, 0, s>>>(pa);
+      break;
+    }
+    case KITES_STRATEGY_PUSH: {
+      chunk_geom<OffT> go{(const OffT *)f.outR, g->outC, f.out_chunks, f.out_nchunks,
+                          g->n, g->n + g->m, g->chunk_items};
+      push_batch_args<OffT> pa{go, g->outE, f.D, Uc, Mc, Un, Mn, g->ctr};
+      k_push_batch<OP, OffT, K><<<f.push_grid, kBlock, 0, s>>>(pa);
+      break;
+    }
+    default:
+      return fail(KITES_ERR_UNSUPPORTED, "strategy %d is not a batched strategy", strategy);
+  }
+  ++*launches;
+  KITES_CUDA_TRY(cudaGetLastError());
+  return KITES_OK;
+}
+
+// Clears what the iteration consumed (the frontier scratch, U[parity] and
+// M[parity]) and runs the loop check.
+int launch_batch_tail(kites_graph *g, const batch_flex &f, int parity,
+                      cudaGraphConditionalHandle h, int hh, uint64_t *launches) {
+  cudaStream_t s = g->eng->stream;
+  k_clear_two<<<grid_for(f.nwords, 256, 4096), 256, 0, s>>>(f.A, f.U[parity], f.nwords);
+  k_clear_words<<<grid_for(g->n, 256, 4096), 256, 0, s>>>(f.M[parity], g->n);
+  iter_record rec{g->rec_active, g->rec_edges, KITES_MAX_RECORDED_ITERS};
+  k_loop_check<<<1, 1, 0, s>>>(g->ctr, rec, h, hh);
+  KITES_CUDA_TRY(cudaGetLastError());
+  *launches += 3;
+  return KITES_OK;
+}
+
+template <int OP, typename OffT, int K>
+int launch_batch_flex_iteration(kites_graph *g, const batch_flex &f, int strategy, int parity,
+                                cudaGraphConditionalHandle h, int hh, uint64_t *launches,
+                                bool time_pull) {
+  cudaStream_t s = g->eng->stream;
+  if (time_pull) KITES_CUDA_TRY(cudaEventRecord(g->eng->kev0, s));
+  KITES_TRY((launch_batch_strategy<OP, OffT, K>(g, f, strategy, parity, launches)));
+  if (time_pull) KITES_CUDA_TRY(cudaEventRecord(g->eng->kev1, s));
+  return launch_batch_tail(g, f, parity, h, hh, launches);
+}
+
+// Device loop of batched AUTO: while (not converged) { select; switch(class)
+// {PLAIN, PUSH, PULL_ALL, PULL_CHANGED}; clear; check } for both parities.
+template <int OP, typename OffT, int K>
+int build_batch_auto_loop(kites_graph *g, const batch_flex &f, float margin,
+                          cudaGraphExec_t *exec) {
+  cudaStream_t s = g->eng->stream;
+  cudaGraph_t graph;
+  KITES_CUDA_TRY(cudaGraphCreate(&graph, 0));
+  cudaGraphConditionalHandle hw;
+  KITES_CUDA_TRY(cudaGraphConditionalHandleCreate(&hw, graph, 1, cudaGraphCondAssignDefault));
+  cudaGraphNodeParams wp = {};
+  wp.type = cudaGraphNodeTypeConditional;
+  wp.conditional.handle = hw;
+  wp.conditional.type = cudaGraphCondTypeWhile;
+  wp.conditional.size = 1;
+  cudaGraphNode_t wnode;
+  KITES_CUDA_TRY(cudaGraphAddNode(&wnode, graph, nullptr, 0, &wp));
+  cudaGraph_t body = wp.conditional.phGraph_out[0];
+  std::vector<cudaGraphNode_t> leaves;
+  uint64_t dummy = 0;
+  for (int parity = 0; parity < 2; ++parity) {
+    cudaGraphConditionalHandle hs;
+    KITES_CUDA_TRY(cudaGraphConditionalHandleCreate(&hs, body, 0, cudaGraphCondAssignDefault));
+    std::vector<cudaGraphNode_t> sel_leaves;
+    KITES_TRY(capture_into(s, body, leaves, [&] {
+      return launch_select<OffT>(g, f.U[parity], margin, nullptr, 0, hs, 1, &dummy,
+                                 g->eng->sel_params_batch);
+    }, &sel_leaves));
+    cudaGraphNodeParams sp = {};
+    sp.type = cudaGraphNodeTypeConditional;
+    sp.conditional.handle = hs;
+    sp.conditional.type = cudaGraphCondTypeSwitch;
+    sp.conditional.size = kClasses;
+    cudaGraphNode_t snode;
+    KITES_CUDA_TRY(cudaGraphAddNode(&snode, body, sel_leaves.data(), sel_leaves.size(), &sp));
+    for (int c = 0; c < kClasses; ++c) {
+      cudaGraph_t branch = sp.conditional.phGraph_out[c];
+      const int strat = batch_class_strategy((uint32_t)c);
+      KITES_TRY(capture_into(s, branch, {}, [&] {
+        return launch_batch_strategy<OP, OffT, K>(g, f, strat, parity, &dummy);
+      }, nullptr));
+    }
+    KITES_TRY(capture_into(s, body, {snode}, [&]() -> int {
+      return launch_batch_tail(g, f, parity, hw, 1, &dummy);
+    }, &leaves));
+  }
+  KITES_CUDA_TRY(cudaGraphInstantiate(exec, graph, 0));
+  g->loops.emplace(loop_key{OP, 3000 + K}, std::make_pair(graph, *exec));
+  return KITES_OK;
+}
+
+// Batched SSSP/BFS with a per-iteration strategy (o.strategy: AUTO, PUSH,
+// PULL_ALL, PULL_CHANGED, or PLAIN through this loop when forced).
+template <int OP, typename OffT, int K>
+int run_batch_flex(kites_graph *g, const uint32_t *sources, uint32_t *dist_out,
+                   const kites_run_opts &o, kites_run_stats *st) {
+  kites_engine *eng = g->eng;
+  cudaStream_t s = eng->stream;
+  auto t0 = std::chrono::steady_clock::now();
+  batch_flex f{};
+  KITES_TRY(prepare_batch_flex<OffT>(g, K, &f));
+  KITES_TRY((size_batch_flex_grids<OP, OffT, K>(g, &f)));
+  const bool autosel = o.strategy == KITES_STRATEGY_AUTO;
+  if (autosel) KITES_TRY(prepare_select(g));
+  KITES_CUDA_TRY(cudaMemcpyAsync(g->d_sources, sources, K * 4, cudaMemcpyDefault, s));
+  k_fill_u32<<<grid_for(g->n * K), 256, 0, s>>>(f.D, g->n * K, kInf);
+  KITES_CUDA_TRY(cudaMemsetAsync(f.A, 0, 4 * f.nwords * 4, s));
+  KITES_CUDA_TRY(cudaMemsetAsync(g->bmask, 0, 2 * g->n * 4, s));
+  k_seed_batch_changed<<<1, 256, 0, s>>>(f.D, K, g->d_sources, f.U[0], f.M[0]);
+  KITES_CUDA_TRY(cudaGetLastError());
+  run_counters c;
+  float ms = 0.f;
+  uint64_t launches = 0;
+  const bool dev_loop = o.device_loop && !o.time_kernels;
+  if (autosel && dev_loop) {
+    // The cached loop bakes in the margin it was captured with.
+    const loop_key key{OP, 3000 + (int)K};
+    auto it = g->loops.find(key);
+    if (it != g->loops.end() && g->auto_margin_batch != o.selector_margin) {
+      cudaGraphExecDestroy(it->second.second);
+      cudaGraphDestroy(it->second.first);
+      g->loops.erase(it);
+      it = g->loops.end();
+    }
+    cudaGraphExec_t ex;
+    if (it == g->loops.end()) {
+      KITES_TRY((build_batch_auto_loop<OP, OffT, K>(g, f, o.selector_margin, &ex)));
+      g->auto_margin_batch = o.selector_margin;
+    } else {
+      ex = it->second.second;
+    }
+    run_counters *hctr = (run_counters *)eng->pinned;
+    *hctr = run_counters{};
+    hctr->max_iterations = o.max_iterations ? o.max_iterations : 2 * g->n + 16;
+    KITES_CUDA_TRY(cudaMemcpyAsync(g->ctr, hctr, sizeof(run_counters), cudaMemcpyHostToDevice, s));
+    KITES_CUDA_TRY(cudaEventRecord(eng->ev0, s));
+    KITES_CUDA_TRY(cudaGraphLaunch(ex, s));
+    KITES_CUDA_TRY(cudaEventRecord(eng->ev1, s));
+    KITES_CUDA_TRY(cudaMemcpyAsync(hctr, g->ctr, sizeof(run_counters), cudaMemcpyDeviceToHost, s));
+    KITES_CUDA_TRY(cudaStreamSynchronize(s));
+    KITES_CUDA_TRY(cudaEventElapsedTime(&ms, eng->ev0, eng->ev1));
+    c = *hctr;
+    launches = 6ull * c.iterations;
+  } else if (autosel) {
+    // Host loop: select, read the class back, run it (timed per iteration).
+    run_counters *hctr = (run_counters *)eng->pinned;
+    *hctr = run_counters{};
+    hctr->max_iterations = o.max_iterations ? o.max_iterations : 2 * g->n + 16;
+    KITES_CUDA_TRY(cudaMemcpyAsync(g->ctr, hctr, sizeof(run_counters), cudaMemcpyHostToDevice, s));
+    KITES_CUDA_TRY(cudaEventRecord(eng->ev0, s));
+    for (uint64_t i = 0;; ++i) {
+      const int parity = (int)(i & 1);
+      KITES_TRY(launch_select<OffT>(g, f.U[parity], o.selector_margin, nullptr, 0, 0, 0,
+                                    &launches, eng->sel_params_batch));
+      KITES_CUDA_TRY(cudaMemcpyAsync(hctr, g->ctr, sizeof(run_counters), cudaMemcpyDeviceToHost, s));
+      KITES_CUDA_TRY(cudaStreamSynchronize(s));
+      const int strat = batch_class_strategy(hctr->sel);
+      KITES_TRY((launch_batch_flex_iteration<OP, OffT, K>(g, f, strat, parity, 0, 0, &launches,
+                                                         o.time_kernels != 0)));
+      KITES_CUDA_TRY(cudaMemcpyAsync(hctr, g->ctr, sizeof(run_counters), cudaMemcpyDeviceToHost, s));
+      KITES_CUDA_TRY(cudaStreamSynchronize(s));
+      if (o.time_kernels && st) {
+        float kms = 0.f;
+        KITES_CUDA_TRY(cudaEventElapsedTime(&kms, eng->kev0, eng->kev1));
+        st->pull_kernel_ms += kms;
+        st->pull_kernel_launches += 1;
+        if (i < KITES_MAX_RECORDED_ITERS) st->iter_ms[i] = kms;
+      }
+      if (hctr->done) break;
+    }
+    KITES_CUDA_TRY(cudaEventRecord(eng->ev1, s));
+    KITES_CUDA_TRY(cudaMemcpyAsync(hctr, g->ctr, sizeof(run_counters), cudaMemcpyDeviceToHost, s));
+    KITES_CUDA_TRY(cudaStreamSynchronize(s));
+    KITES_CUDA_TRY(cudaEventElapsedTime(&ms, eng->ev0, eng->ev1));
+    c = *hctr;
+  } else {
+    const int strategy = o.strategy;
+    auto launch = [g, &f, strategy](int parity, cudaGraphConditionalHandle h, int hh,
+                                    uint64_t *l, bool tp) {
+      return launch_batch_flex_iteration<OP, OffT, K>(g, f, strategy, parity, h, hh, l, tp);
+    };
+    KITES_TRY(drive_loop(g, o, loop_key{OP, 2000 + 16 * strategy + (int)(K / 16)}, launch, &c,
+                         &ms, &launches, st));
+  }
+  if (dist_out) {
+    KITES_CUDA_TRY(cudaMemcpyAsync(dist_out, f.D, g->n_given * K * 4, cudaMemcpyDefault, s));
+    KITES_CUDA_TRY(cudaStreamSynchronize(s));
+  }
+  if (st) {
+    st->iterations = c.iterations;
+    st->device_ms = ms;
+    st->edges_traversed = c.total_edges;
+    const uint64_t e_bytes = op_reads_weights<OP>() ? 4 : 0;
+    // Bytes as the unmasked pull would move them (an upper bound for the
+    // masked strategies, which skip unchanged sectors).
+    st->algorithmic_bytes = c.iterations * 8ull * f.nwords + (8ull + 4ull * K) * c.total_active +
+                            (4ull + e_bytes + 4ull * K) * c.total_edges +
+                            (4ull * K + 8ull) * c.total_updated + 8ull * c.total_out_edges;
+    const uint32_t nrec =
+        (uint32_t)std::min<unsigned long long>(c.iterations, KITES_MAX_RECORDED_ITERS);
+    std::vector<uint8_t> cls(nrec, 0);
+    if (autosel && nrec)
+      KITES_CUDA_TRY(cudaMemcpy(cls.data(), g->rec_sel, nrec, cudaMemcpyDeviceToHost));
+    for (uint32_t i = 0; i < nrec; ++i)
+      st->strategy_hist[autosel ? batch_class_strategy(cls[i]) : o.strategy] += 1;
+    st->kernel_launches += launches + 3;
+    if (o.record_iterations) {
+      KITES_TRY(record_iterations(g, c, o.strategy, st));
+      for (uint32_t i = 0; i < nrec && i < st->n_recorded; ++i)
+        st->iter_strategy[i] = (uint8_t)(autosel ? batch_class_strategy(cls[i]) : o.strategy);
+    }
+    st->host_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  }
+  if (c.error) return run_error(c.error);
+  if (c.timed_out)
+    return fail(KITES_ERR_TIMEOUT, "no fixed point after %llu iterations",
+                (unsigned long long)c.iterations);
+  return KITES_OK;
+}
+
+// Training data for the batched selector: from the state at the start of
+// every iteration, each class runs once (timed with CUDA events) and the
+// state (D, U, M, counters) is restored; then the loop advances with PLAIN.
+template <int OP, typename OffT, int K>
+int record_batch_classes(kites_graph *g, const uint32_t *sources, float *feat, float *times,
+                         uint32_t cap, uint32_t *n_out) {
+  kites_engine *eng = g->eng;
+  cudaStream_t s = eng->stream;
+  batch_flex f{};
+  KITES_TRY(prepare_batch_flex<OffT>(g, K, &f));
+  KITES_TRY((size_batch_flex_grids<OP, OffT, K>(g, &f)));
+  KITES_TRY(prepare_select(g));
+  KITES_CUDA_TRY(cudaMemcpyAsync(g->d_sources, sources, K * 4, cudaMemcpyDefault, s));
+  k_fill_u32<<<grid_for(g->n * K), 256, 0, s>>>(f.D, g->n * K, kInf);
+  KITES_CUDA_TRY(cudaMemsetAsync(f.A, 0, 4 * f.nwords * 4, s));
+  KITES_CUDA_TRY(cudaMemsetAsync(g->bmask, 0, 2 * g->n * 4, s));
+  k_seed_batch_changed<<<1, 256, 0, s>>>(f.D, K, g->d_sources, f.U[0], f.M[0]);
+  KITES_CUDA_TRY(cudaGetLastError());
+  void *p;
+  KITES_TRY(dev_alloc(eng, &p, (uint64_t)cap * kFeat * 4));
+  float *dfeat = (float *)p;
+  const size_t dbytes = g->n * (size_t)K * 4, bbytes = 4 * f.nwords * 4, mbytes = 2 * g->n * 4;
+  int st = dev_alloc(eng, &p, dbytes + bbytes + mbytes + sizeof(run_counters));
+  if (st != KITES_OK) {
+    cudaFreeAsync(dfeat, s);
+    return st;
+  }
+  uint8_t *snap = (uint8_t *)p;
+  run_counters *snapC = (run_counters *)(snap + dbytes + bbytes + mbytes);
+  run_counters *hctr = (run_counters *)eng->pinned;
+  *hctr = run_counters{};
+  hctr->max_iterations = 2 * g->n + 16;
+  cudaMemcpyAsync(g->ctr, hctr, sizeof(run_counters), cudaMemcpyHostToDevice, s);
+  auto save = [&](bool restore) {
+    auto cp = [&](void *a, void *b, size_t n) {
+      if (restore) cudaMemcpyAsync(a, b, n, cudaMemcpyDeviceToDevice, s);
+      else cudaMemcpyAsync(b, a, n, cudaMemcpyDeviceToDevice, s);
+    };
+    cp(f.D, snap, dbytes);
+    cp(f.A, snap + dbytes, bbytes);
+    cp(g->bmask, snap + dbytes + bbytes, mbytes);
+    cp(g->ctr, snapC, sizeof(run_counters));
+  };
+  uint64_t launches = 0;
+  uint32_t n = 0;
+  for (uint64_t i = 0; i < cap; ++i) {
+    const int parity = (int)(i & 1);
+    if ((st = launch_select<OffT>(g, f.U[parity], 0.f, dfeat, cap, 0, 0, &launches,
+                                  eng->sel_params_batch)) != KITES_OK)
+      break;
+    save(false);
+    for (uint32_t c = 0; c < (uint32_t)kClasses; ++c) {
+      cudaEventRecord(eng->kev0, s);
+      st = launch_batch_strategy<OP, OffT, K>(g, f, batch_class_strategy(c), parity, &launches);
+      cudaEventRecord(eng->kev1, s);
+      if (st != KITES_OK) break;
+      save(true);
+      cudaError_t e = cudaStreamSynchronize(s);
+      if (e != cudaSuccess) { st = fail(KITES_ERR_CUDA, "record: %s", cudaGetErrorString(e)); break; }
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, eng->kev0, eng->kev1);
+      times[(uint64_t)n * kClasses + c] = ms;
+    }
+    if (st != KITES_OK) break;
+    if ((st = launch_batch_flex_iteration<OP, OffT, K>(g, f, KITES_STRATEGY_PLAIN, parity, 0, 0,
+                                                       &launches, false)) != KITES_OK)
+      break;
+    cudaMemcpyAsync(hctr, g->ctr, sizeof(run_counters), cudaMemcpyDeviceToHost, s);
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) { st = fail(KITES_ERR_CUDA, "record: %s", cudaGetErrorString(e)); break; }
+    ++n;
+    if (hctr->done) break;
+  }
+  if (st == KITES_OK && n) {
+    cudaError_t e = cudaMemcpy(feat, dfeat, (uint64_t)n * kFeat * 4, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) st = fail(KITES_ERR_CUDA, "record copy: %s", cudaGetErrorString(e));
+  }
+  cudaFreeAsync(dfeat, s);
+  cudaFreeAsync(snap, s);
+  cudaStreamSynchronize(s);
+  *n_out = n;
+  return st;
+}
+
+template <int OP, typename OffT>
+int dispatch_batch_flex_k(kites_graph *g, const uint32_t *src, uint32_t k, uint32_t *out,
+                          const kites_run_opts &o, kites_run_stats *st) {
+  switch (k) {
+    case 16: return run_batch_flex<OP, OffT, 16>(g, src, out, o, st);
+    case 32: return run_batch_flex<OP, OffT, 32>(g, src, out, o, st);
+    case 64: return run_batch_flex<OP, OffT, 64>(g, src, out, o, st);
+    case 128: return run_batch_flex<OP, OffT, 128>(g, src, out, o, st);
+    case 256: return run_batch_flex<OP, OffT, 256>(g, src, out, o, st);
+    default: return fail(KITES_ERR_INVALID, "batch size %u is not 16, 32, 64, 128 or 256", k);
+  }
+}
+
+template <typename OffT>
+int dispatch_batch_flex(kites_graph *g, int op, const uint32_t *src, uint32_t k, uint32_t *out,
+                        const kites_run_opts &o, kites_run_stats *st) {
+  switch (op) {
+    case OP_SSSP: return dispatch_batch_flex_k<OP_SSSP, OffT>(g, src, k, out, o, st);
+    case OP_BFS: return dispatch_batch_flex_k<OP_BFS, OffT>(g, src, k, out, o, st);
+    default:
+      return fail(KITES_ERR_UNSUPPORTED,
+                  "batched strategies other than PLAIN take the saturating SSSP or BFS");
+  }
+}
+
+template <int OP, typename OffT>
+int dispatch_record_batch_k(kites_graph *g, const uint32_t *src, uint32_t k, float *feat,
+                            float *times, uint32_t cap, uint32_t *n_out) {
+  switch (k) {
+    case 16: return record_batch_classes<OP, OffT, 16>(g, src, feat, times, cap, n_out);
+    case 32: return record_batch_classes<OP, OffT, 32>(g, src, feat, times, cap, n_out);
+    case 64: return record_batch_classes<OP, OffT, 64>(g, src, feat, times, cap, n_out);
+    case 128: return record_batch_classes<OP, OffT, 128>(g, src, feat, times, cap, n_out);
+    case 256: return record_batch_classes<OP, OffT, 256>(g, src, feat, times, cap, n_out);
+    default: return fail(KITES_ERR_INVALID, "batch size %u is not 16, 32, 64, 128 or 256", k);
+  }
+}
+
 int check_graph(kites_engine *eng, kites_graph *g) {
   if (!eng || !g) return fail(KITES_ERR_INVALID, "null engine or graph");
   if (g->eng != eng) return fail(KITES_ERR_INVALID, "graph belongs to another engine");
@@ -1494,6 +1988,21 @@ extern "C" int kites_engine_create(int device, kites_engine **out) {
 #else
     k_mlp_neutral<<<1, 256, 0, eng->stream>>>(eng->sel_params);
 #endif
+    if ((ce = cudaMalloc((void **)&eng->sel_params_batch, kParams * sizeof(float))) !=
+        cudaSuccess) {
+      st = fail(KITES_ERR_OOM, "selector allocation failed: %s", cudaGetErrorString(ce));
+      break;
+    }
+#ifdef KITES_HAVE_DEFAULT_BATCH_SELECTOR
+    ce = cudaMemcpyAsync(eng->sel_params_batch, kDefaultBatchSelector,
+                         sizeof(kDefaultBatchSelector), cudaMemcpyHostToDevice, eng->stream);
+    if (ce != cudaSuccess) {
+      st = fail(KITES_ERR_CUDA, "selector init failed: %s", cudaGetErrorString(ce));
+      break;
+    }
+#else
+    k_mlp_neutral<<<1, 256, 0, eng->stream>>>(eng->sel_params_batch);
+#endif
     if ((ce = cudaStreamSynchronize(eng->stream)) != cudaSuccess) {
       st = fail(KITES_ERR_CUDA, "selector init failed: %s", cudaGetErrorString(ce));
       break;
@@ -1515,6 +2024,7 @@ extern "C" int kites_engine_destroy(kites_engine *eng) {
   while (!eng->graphs.empty()) kites_graph_destroy(eng->graphs.back());
   if (eng->pinned) cudaFreeHost(eng->pinned);
   if (eng->sel_params) cudaFree(eng->sel_params);
+  if (eng->sel_params_batch) cudaFree(eng->sel_params_batch);
   if (eng->ev0) cudaEventDestroy(eng->ev0);
   if (eng->ev1) cudaEventDestroy(eng->ev1);
   if (eng->kev0) cudaEventDestroy(eng->kev0);
@@ -1689,8 +2199,8 @@ extern "C" int kites_graph_from_edges(kites_engine *eng, uint64_t n_vertices, ui
   if (n_vertices == 0 || n_vertices >= 0xFFFFFF00ull)
     return fail(KITES_ERR_INVALID, "n_vertices must be in 1 .. 2^32 - 256");
   if (n_edges && (!src || !dst)) return fail(KITES_ERR_INVALID, "null edge arrays");
-  if (n_edges > 0x7FFFFFFFull)
-    return fail(KITES_ERR_UNSUPPORTED, "device ingestion takes < 2^31 edges");
+  if (n_edges > 0xFFFFFFFFull)
+    return fail(KITES_ERR_UNSUPPORTED, "device ingestion takes < 2^32 edges");
   KITES_TRY(set_device(eng));
   cudaStream_t s = eng->stream;
   const uint64_t m = n_edges, n = n_vertices;
@@ -1744,23 +2254,31 @@ extern "C" int kites_graph_from_edges(kites_engine *eng, uint64_t n_vertices, ui
       size_t temp_bytes = 0;
       if (weights)
         e = cub::DeviceRadixSort::SortPairs(nullptr, temp_bytes, keys[0], keys[1], w[0], w[1],
-                                            (int)m, 0, end_bit, s);
+                                            (uint64_t)m, 0, end_bit, s);
       else
-        e = cub::DeviceRadixSort::SortKeys(nullptr, temp_bytes, keys[0], keys[1], (int)m, 0,
+        e = cub::DeviceRadixSort::SortKeys(nullptr, temp_bytes, keys[0], keys[1], (uint64_t)m, 0,
                                            end_bit, s);
       if (e != cudaSuccess) { st = fail(KITES_ERR_CUDA, "sort: %s", cudaGetErrorString(e)); break; }
       if ((st = alloc(&temp, temp_bytes)) != KITES_OK) break;
       if (weights)
         e = cub::DeviceRadixSort::SortPairs(temp, temp_bytes, keys[0], keys[1], w[0], w[1],
-                                            (int)m, 0, end_bit, s);
+                                            (uint64_t)m, 0, end_bit, s);
       else
-        e = cub::DeviceRadixSort::SortKeys(temp, temp_bytes, keys[0], keys[1], (int)m, 0,
+        e = cub::DeviceRadixSort::SortKeys(temp, temp_bytes, keys[0], keys[1], (uint64_t)m, 0,
                                            end_bit, s);
       if (e != cudaSuccess) { st = fail(KITES_ERR_CUDA, "sort: %s", cudaGetErrorString(e)); break; }
     }
     k_rows_of_keys<<<grid_for(n + 1), 256, 0, s>>>(keys[1], m, n, R, C);
     e = cudaGetLastError();
     if (e != cudaSuccess) { st = fail(KITES_ERR_CUDA, "rows: %s", cudaGetErrorString(e)); break; }
+    // The keys (16 bytes an edge), the unsorted weights and the sort's
+    // scratch go back to the pool before the upload builds the graph's own
+    // arrays: at 2^31 edges that is about 50 GB less at the peak.
+    for (void *q : {(void *)keys[0], (void *)keys[1], (void *)w[0], temp}) {
+      if (!q) continue;
+      cudaFreeAsync(q, s);
+      tmp.erase(std::remove(tmp.begin(), tmp.end(), q), tmp.end());
+    }
     kites_csc_view v = {};
     v.n_vertices = n;
     v.n_edges = m;
@@ -1981,6 +2499,14 @@ extern "C" int kites_sssp_batch(kites_engine *eng, kites_graph *g, int op,
       return fail(KITES_ERR_INVALID, "source %u (slot %u) out of range", host_src[i], i);
   kites_run_opts o = resolve_opts(opts);
   if (stats) memset(stats, 0, sizeof(*stats));
+  if (o.strategy != KITES_STRATEGY_PLAIN) {
+    if (o.strategy != KITES_STRATEGY_AUTO && o.strategy != KITES_STRATEGY_PUSH &&
+        o.strategy != KITES_STRATEGY_PULL_ALL && o.strategy != KITES_STRATEGY_PULL_CHANGED)
+      return fail(KITES_ERR_UNSUPPORTED, "strategy %d is not a batched strategy", o.strategy);
+    if (!g->outE) return fail(KITES_ERR_UNSUPPORTED, "graph has no weighted out-CSR");
+    return g->off64 ? dispatch_batch_flex<uint64_t>(g, op, host_src, k, dist_out, o, stats)
+                    : dispatch_batch_flex<uint32_t>(g, op, host_src, k, dist_out, o, stats);
+  }
   return g->off64 ? dispatch_batch<uint64_t>(g, op, host_src, k, dist_out, o, stats)
                   : dispatch_batch<uint32_t>(g, op, host_src, k, dist_out, o, stats);
 }
@@ -2062,10 +2588,27 @@ extern "C" int kites_selector_record(kites_engine *eng, kites_graph *g, int op, 
                   : dispatch_record<uint32_t>(g, op, features, times_ms, capacity, n_records);
 }
 
+static int fit_selector(kites_engine *eng, const float *features, const float *times_ms,
+                        uint32_t n, uint32_t epochs, float lr, uint64_t seed, float *params_out,
+                        float *final_loss, bool load);
+
 extern "C" int kites_selector_train(kites_engine *eng, const float *features,
                                     const float *times_ms, uint32_t n, uint32_t epochs,
                                     float lr, uint64_t seed, float *params_out,
                                     float *final_loss) {
+  return fit_selector(eng, features, times_ms, n, epochs, lr, seed, params_out, final_loss, true);
+}
+
+extern "C" int kites_selector_fit(kites_engine *eng, const float *features,
+                                  const float *times_ms, uint32_t n, uint32_t epochs, float lr,
+                                  uint64_t seed, float *params_out, float *final_loss) {
+  if (!params_out) return fail(KITES_ERR_INVALID, "null params_out");
+  return fit_selector(eng, features, times_ms, n, epochs, lr, seed, params_out, final_loss, false);
+}
+
+static int fit_selector(kites_engine *eng, const float *features, const float *times_ms,
+                        uint32_t n, uint32_t epochs, float lr, uint64_t seed, float *params_out,
+                        float *final_loss, bool load) {
   clear_error();
   if (!eng || !features || !times_ms || n == 0) return fail(KITES_ERR_INVALID, "bad arguments");
   KITES_TRY(set_device(eng));
@@ -2094,13 +2637,66 @@ extern "C" int kites_selector_train(kites_engine *eng, const float *features,
     k_mlp_adam<<<(kParams + 255) / 256, 256, 0, s>>>(P, G, M, Vv, lr, 0.9f, 0.999f, 1e-8f, (int)e);
   }
   KITES_CUDA_TRY(cudaGetLastError());
-  KITES_CUDA_TRY(cudaMemcpyAsync(eng->sel_params, P, kParams * 4, cudaMemcpyDeviceToDevice, s));
+  if (load)
+    KITES_CUDA_TRY(cudaMemcpyAsync(eng->sel_params, P, kParams * 4, cudaMemcpyDeviceToDevice, s));
   float hloss = 0.f;
   KITES_CUDA_TRY(cudaMemcpyAsync(&hloss, loss, 4, cudaMemcpyDeviceToHost, s));
   if (params_out) KITES_CUDA_TRY(cudaMemcpyAsync(params_out, P, kParams * 4, cudaMemcpyDefault, s));
   KITES_CUDA_TRY(cudaFreeAsync(p, s));
   KITES_CUDA_TRY(cudaStreamSynchronize(s));
   if (final_loss) *final_loss = hloss;
+  return KITES_OK;
+}
+
+extern "C" int kites_selector_record_batch(kites_engine *eng, kites_graph *g, int op,
+                                           const uint32_t *sources, uint32_t k, float *features,
+                                           float *times_ms, uint32_t capacity,
+                                           uint32_t *n_records) {
+  clear_error();
+  KITES_TRY(check_graph(eng, g));
+  if (!sources || !features || !times_ms || !n_records || capacity == 0)
+    return fail(KITES_ERR_INVALID, "null argument or zero capacity");
+  if (op != OP_SSSP && op != OP_BFS) return fail(KITES_ERR_INVALID, "recording takes SSSP or BFS");
+  if (op == OP_SSSP && g->esize != 4) return fail(KITES_ERR_UNSUPPORTED, "SSSP needs 4-byte edges");
+  if (k != 16 && k != 32 && k != 64 && k != 128 && k != 256)
+    return fail(KITES_ERR_INVALID, "batch size %u is not 16, 32, 64, 128 or 256", k);
+  uint32_t hs[256];
+  KITES_CUDA_TRY(cudaMemcpy(hs, sources, k * 4, cudaMemcpyDefault));
+  for (uint32_t i = 0; i < k; ++i)
+    if (hs[i] >= g->n_given) return fail(KITES_ERR_INVALID, "source %u out of range", hs[i]);
+  if (op == OP_SSSP)
+    return g->off64 ? dispatch_record_batch_k<OP_SSSP, uint64_t>(g, hs, k, features, times_ms,
+                                                                 capacity, n_records)
+                    : dispatch_record_batch_k<OP_SSSP, uint32_t>(g, hs, k, features, times_ms,
+                                                                 capacity, n_records);
+  return g->off64 ? dispatch_record_batch_k<OP_BFS, uint64_t>(g, hs, k, features, times_ms,
+                                                              capacity, n_records)
+                  : dispatch_record_batch_k<OP_BFS, uint32_t>(g, hs, k, features, times_ms,
+                                                              capacity, n_records);
+}
+
+extern "C" int kites_selector_load_batch(kites_engine *eng, const float *params,
+                                         uint32_t n_params) {
+  clear_error();
+  if (!eng || !params) return fail(KITES_ERR_INVALID, "null argument");
+  if (n_params != (uint32_t)kParams)
+    return fail(KITES_ERR_INVALID, "selector has %d parameters, got %u", kParams, n_params);
+  KITES_TRY(set_device(eng));
+  KITES_CUDA_TRY(cudaMemcpyAsync(eng->sel_params_batch, params, kParams * 4, cudaMemcpyDefault,
+                                 eng->stream));
+  KITES_CUDA_TRY(cudaStreamSynchronize(eng->stream));
+  return KITES_OK;
+}
+
+extern "C" int kites_selector_save_batch(kites_engine *eng, float *params, uint32_t n_params) {
+  clear_error();
+  if (!eng || !params) return fail(KITES_ERR_INVALID, "null argument");
+  if (n_params != (uint32_t)kParams)
+    return fail(KITES_ERR_INVALID, "selector has %d parameters, got %u", kParams, n_params);
+  KITES_TRY(set_device(eng));
+  KITES_CUDA_TRY(cudaMemcpyAsync(params, eng->sel_params_batch, kParams * 4, cudaMemcpyDefault,
+                                 eng->stream));
+  KITES_CUDA_TRY(cudaStreamSynchronize(eng->stream));
   return KITES_OK;
 }
 

@@ -19,6 +19,7 @@ struct kites_engine {
   int l2_bytes = 0;
   void *pinned = nullptr;         // small pinned scratch for flag read-backs
   float *sel_params = nullptr;    // learned selector weights (device), or null
+  float *sel_params_batch = nullptr;  // the batched loop's selector weights
   std::vector<struct kites_graph *> graphs;   // live graphs, destroyed with the engine
 };
 
@@ -101,11 +102,14 @@ struct kites_graph {
   const void *dmap_ptr = nullptr;
   uint32_t dmap_K = 0;
   int batch_gather = 0;
+  uint32_t *bmask = nullptr;         // batched strategies: changed sectors per vertex,
+                                     // two parities of n words
   uint32_t *queue = nullptr;         // compacted changed queue (PUSH), n slots
   void *sacc = nullptr;              // selector frontier-count accumulators
   uint8_t *rec_sel = nullptr;        // selector class per iteration (device)
   int tpv_strategy = KITES_STRATEGY_TPV8;   // the selector's threads-per-vertex class
   float auto_margin = -1.f;          // margin the cached AUTO loop was captured with
+  float auto_margin_batch = -1.f;    // the same for the batched AUTO loops
 
   // PageRank scratch (allocated on first use).
   float *pr_x = nullptr, *pr_y = nullptr, *pr_inv_out = nullptr;

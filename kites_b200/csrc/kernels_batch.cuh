@@ -12,6 +12,18 @@
 // K = 64).  The lane groups' minima of a row meet over shuffles.  A vertex
 // whose in-edges span several chunks merges its partial rows with
 // atomicMin, like the single-source kernel.
+//
+// Changed sectors.  A lane's 8 values are one 32-byte sector of a row; the
+// pulls and the push record, per vertex, which sectors of its row they
+// lowered (M, one bit per sector, K/8 bits).  The masked pull gathers of an
+// in-neighbour's row only the sectors that changed in the previous
+// iteration (in-edges from a source with no changed sector cost no gather
+// at all), and the push relaxes only those.  That is exact: after every
+// iteration each edge (u, v) and column k either has u's sector of k marked
+// or already satisfies D[v][k] <= nbrComp(D[u][k], w) -- a pull or push that
+// reads D[u][k] establishes it, a later change of D[u][k] marks the sector
+// again, and values only decrease.  It needs a monotone nbrComp, so the
+// masked strategies take the saturating operators (SSSP, BFS).
 #pragma once
 #include "kernels.cuh"
 
@@ -22,6 +34,8 @@ struct batch_shape {
   static constexpr int VPL = 8;          // values per lane: one 32-byte access
   static constexpr int LPE = K / VPL;    // lanes per edge (a K-wide row)
   static constexpr int EPW = 32 / LPE;   // edges per warp step
+  // Sector bits of a row (bit kl = lane kl's 8 values).
+  static constexpr uint32_t kSectors = LPE == 32 ? kFull : ((1u << LPE) - 1u);
   static_assert(K == 16 || K == 32 || K == 64 || K == 128 || K == 256, "K");
 };
 
@@ -66,6 +80,14 @@ __device__ __forceinline__ void load_row8(const uint32_t *p, uint32_t (&x)[8]) {
                  "=r"(x[6]), "=r"(x[7])
                : "l"(p));
 }
+// The same 32 bytes through L1: the push reads one source row for each of
+// its out-edges, so the repeats hit.
+__device__ __forceinline__ void load_row8_l1(const uint32_t *p, uint32_t (&x)[8]) {
+  asm volatile("ld.global.v8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+               : "=r"(x[0]), "=r"(x[1]), "=r"(x[2]), "=r"(x[3]), "=r"(x[4]), "=r"(x[5]),
+                 "=r"(x[6]), "=r"(x[7])
+               : "l"(p));
+}
 __device__ __forceinline__ void store_row8(uint32_t *p, const uint32_t (&x)[8]) {
   asm volatile("st.global.v8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};"
                :: "l"(p), "r"(x[0]), "r"(x[1]), "r"(x[2]), "r"(x[3]), "r"(x[4]), "r"(x[5]),
@@ -84,19 +106,25 @@ struct pull_batch_args {
   chunk_geom<OffT> g;
   const uint32_t *E;
   uint32_t *D;            // n x K
-  const uint32_t *rd;     // read frontier (vertex bits)
+  const uint32_t *rd;     // read frontier (vertex bits); null = every row
   uint32_t *chg;          // changed vertices
   run_counters *ctr;
+  const uint32_t *Mprev;  // masked pull: changed sectors of the previous iteration
+  uint32_t *Mnext;        // sectors this pull lowers, or null
 };
 
 // Four CTAs (32 warps) per SM keep more source rows in flight than fewer,
-// fatter warps; K = 256 rows need the registers of two.
-template <int OP, typename OffT, int K>
+// fatter warps; K = 256 rows need the registers of two.  kMasked: gather
+// only the changed sectors of each in-neighbour's row (a.Mprev); the live
+// in-edges of a 32-edge tile are packed first so that lane groups take
+// only edges that gather something.
+template <int OP, typename OffT, int K, bool kMasked = false>
 __global__ void __launch_bounds__(kBlock, K >= 256 ? 2 : 4)
     k_pull_batch(pull_batch_args<OffT> a) {
   if (a.ctr->done) return;
   using S = batch_shape<K>;
   constexpr int kRowsInFlight = rows_in_flight<K>();
+  __shared__ uint8_t s_slot[kWarpsPerBlock][32];   // masked: lane of the j-th live edge
   const uint32_t lane = lane_id(), wib = threadIdx.x >> 5;
   const uint32_t sub = lane / S::LPE, kl = lane % S::LPE;
   unsigned long long n_act = 0, n_edges = 0, n_chg = 0;
@@ -109,7 +137,7 @@ __global__ void __launch_bounds__(kBlock, K >= 256 ? 2 : 4)
     uint64_t v_last = a.g.chunk_v0[ch + 1];
     if (v_last >= a.g.n_rows) v_last = a.g.n_rows - 1;
     for (uint64_t vb = v_first & ~31ull; vb <= v_last; vb += 32) {
-      uint32_t mask = a.rd[vb >> 5];
+      uint32_t mask = a.rd ? a.rd[vb >> 5] : kFull;
       if (vb < v_first) mask &= kFull << (uint32_t)(v_first - vb);
       if (v_last - vb < 31) mask &= kFull >> (31u - (uint32_t)(v_last - vb));
       uint32_t upd_bits = 0;
@@ -128,13 +156,22 @@ __global__ void __launch_bounds__(kBlock, K >= 256 ? 2 : 4)
         uint32_t acc[S::VPL];
 #pragma unroll
         for (int q = 0; q < S::VPL; ++q) acc[q] = kInf;
+        bool row_live = !kMasked;
         for (int64_t tile = lo; tile < hi; tile += 32) {
           const int64_t t = tile + lane;
-          const uint32_t ntile = (uint32_t)min((int64_t)32, hi - tile);
-          uint32_t cC = 0, cE = 0;
+          uint32_t ntile = (uint32_t)min((int64_t)32, hi - tile);
+          uint32_t cC = 0, cE = 0, cM = 0;
           if (t < hi) {
             cC = __ldcs(a.g.C + t);
             if (op_reads_weights<OP>()) cE = __ldcs(a.E + t);
+          }
+          if constexpr (kMasked) {
+            cM = t < hi ? a.Mprev[cC] : 0u;
+            const uint32_t live = __ballot_sync(kFull, cM != 0u);
+            if (cM) s_slot[wib][__popc(live & ((1u << lane) - 1u))] = (uint8_t)lane;
+            __syncwarp();
+            ntile = __popc(live);
+            row_live = row_live || live != 0u;
           }
           // kRowsInFlight source rows per lane group are loaded before any
           // is folded.
@@ -143,9 +180,13 @@ __global__ void __launch_bounds__(kBlock, K >= 256 ? 2 : 4)
 #pragma unroll
             for (int r = 0; r < kRowsInFlight; ++r) {
               const uint32_t j = jj + r * S::EPW + sub;
-              const uint32_t u = __shfl_sync(kFull, cC, j & 31u);
-              wq[r] = __shfl_sync(kFull, cE, j & 31u);
-              if (j < ntile) {
+              const uint32_t src = kMasked ? (j < ntile ? (uint32_t)s_slot[wib][j] : 0u)
+                                           : (j & 31u);
+              const uint32_t u = __shfl_sync(kFull, cC, src);
+              wq[r] = __shfl_sync(kFull, cE, src);
+              bool take = j < ntile;
+              if constexpr (kMasked) take = take && ((__shfl_sync(kFull, cM, src) >> kl) & 1u);
+              if (take) {
                 load_row8(a.D + (uint64_t)u * K + kl * S::VPL, row[r]);
               } else {
 #pragma unroll
@@ -159,7 +200,9 @@ __global__ void __launch_bounds__(kBlock, K >= 256 ? 2 : 4)
               for (int q = 0; q < S::VPL; ++q) acc[q] = min(acc[q], nbr_comp<OP>(row[r][q], wq[r]));
             }
           }
+          if constexpr (kMasked) __syncwarp();  // s_slot is rewritten by the next tile
         }
+        if (!row_live) continue;  // masked: no in-neighbour changed
 #pragma unroll
         for (int d = S::LPE; d < 32; d <<= 1) {
 #pragma unroll
@@ -183,7 +226,12 @@ __global__ void __launch_bounds__(kBlock, K >= 256 ? 2 : 4)
               if (acc[q] < cur[q] && acc[q] < atomicMin(dv + q, acc[q])) lane_upd = true;
           }
         }
-        if (__any_sync(kFull, lane_upd)) upd_bits |= 1u << b;
+        // Lanes 0 .. LPE-1 (lane group 0) own the row's sectors.
+        const uint32_t sec = __ballot_sync(kFull, lane_upd) & S::kSectors;
+        if (sec) {
+          upd_bits |= 1u << b;
+          if (a.Mnext && lane == 0) atomicOr(a.Mnext + v, sec);
+        }
       }
       if (upd_bits && lane == 0) {
         n_chg += __popc(upd_bits & ~atomicOr(a.chg + (vb >> 5), upd_bits));
@@ -196,6 +244,136 @@ __global__ void __launch_bounds__(kBlock, K >= 256 ? 2 : 4)
     if (n_edges) atomicAdd(&a.ctr->edges, n_edges);
     if (n_chg) atomicAdd(&a.ctr->changed, n_chg);
   }
+}
+
+// ---- masked push ---------------------------------------------------------
+
+template <typename OffT>
+struct push_batch_args {
+  chunk_geom<OffT> g;     // out-CSR: rows are sources, C their targets
+  const uint32_t *outE;   // weights in out-CSR order
+  uint32_t *D;            // n x K
+  const uint32_t *U;      // rows changed by the previous iteration
+  const uint32_t *Mprev;  // their changed sectors
+  uint32_t *chg;          // next changed set
+  uint32_t *Mnext;        // sectors lowered here
+  run_counters *ctr;
+};
+
+// Sparse changed sets: the out-edges of the changed rows, walked over the
+// out-CSR's edge-balanced chunks (as k_expand_chunked walks them); a lane
+// group takes one out-edge (u, v) and, for each changed sector of u, lowers
+// D[v]'s sector with atomicMin where nbrComp(D[u], w) beats it.
+template <int OP, typename OffT, int K>
+__global__ void __launch_bounds__(kBlock) k_push_batch(push_batch_args<OffT> a) {
+  if (a.ctr->done) return;
+  using S = batch_shape<K>;
+  __shared__ uint32_t s_ex[kWarpsPerBlock][32];
+  __shared__ OffT s_lo[kWarpsPerBlock][32];
+  const uint32_t lane = lane_id(), wib = threadIdx.x >> 5;
+  const uint32_t sub = lane / S::LPE, kl = lane % S::LPE;
+  uint32_t *ex = s_ex[wib];
+  OffT *lo_s = s_lo[wib];
+  unsigned long long n_rows = 0, n_edges = 0, n_chg = 0;
+  bool any = false;
+  const uint64_t stride = (uint64_t)gridDim.x * kWarpsPerBlock;
+  for (uint64_t ch = (uint64_t)blockIdx.x * kWarpsPerBlock + wib; ch < a.g.nchunks;
+       ch += stride) {
+    const int64_t item_lo = (int64_t)(ch * a.g.chunk_items);
+    const int64_t item_hi = min(item_lo + (int64_t)a.g.chunk_items, (int64_t)a.g.n_items);
+    const uint64_t r_first = a.g.chunk_v0[ch];
+    uint64_t r_last = a.g.chunk_v0[ch + 1];
+    if (r_last >= a.g.n_rows) r_last = a.g.n_rows - 1;
+    for (uint64_t rb = r_first & ~31ull; rb <= r_last; rb += 32) {
+      const uint32_t word = a.U[rb >> 5];
+      if (word == 0) continue;
+      const uint64_t r = rb + lane;
+      const bool active = r >= r_first && r <= r_last && ((word >> lane) & 1u);
+      uint32_t cnt = 0;
+      OffT elo = 0;
+      if (active) {
+        const int64_t r0 = (int64_t)a.g.R[r], r1 = (int64_t)a.g.R[r + 1];
+        const int64_t lo = max(r0, item_lo - (int64_t)r - 1);
+        const int64_t hi = min(r1, item_hi - (int64_t)r - 1);
+        cnt = hi > lo ? (uint32_t)(hi - lo) : 0u;
+        elo = (OffT)lo;
+        const int64_t rpos = (int64_t)r + r0;
+        n_rows += (rpos >= item_lo && rpos < item_hi) ? 1u : 0u;
+        n_edges += cnt;
+      }
+      const uint32_t incl = warp_inclusive_scan(cnt);
+      const uint32_t total = __shfl_sync(kFull, incl, 31);
+      if (total == 0) continue;
+      ex[lane] = incl - cnt;
+      lo_s[lane] = elo;
+      __syncwarp();
+      for (uint32_t base = 0; base < total; base += 32) {
+        // Lane i loads virtual out-edge base + i: target, weight, source row
+        // and the source's changed sectors.
+        const uint32_t i = base + lane;
+        uint32_t tv = 0, tw = 0, tr = 0, tm = 0;
+        if (i < total) {
+          const uint32_t j = owner_of(ex, i);
+          const OffT e = lo_s[j] + (OffT)(i - ex[j]);
+          tv = __ldcs(a.g.C + e);
+          if (op_reads_weights<OP>()) tw = __ldcs(a.outE + e);
+          tr = (uint32_t)(rb + j);
+          tm = a.Mprev[tr];
+        }
+        const uint32_t nwin = min(32u, total - base);
+        for (uint32_t s0 = 0; s0 < nwin; s0 += S::EPW) {
+          const uint32_t sl = (s0 + sub) & 31u;
+          const uint32_t v = __shfl_sync(kFull, tv, sl);
+          const uint32_t w = __shfl_sync(kFull, tw, sl);
+          const uint32_t u = __shfl_sync(kFull, tr, sl);
+          const uint32_t mu = __shfl_sync(kFull, tm, sl);
+          bool lowered = false;
+          if (s0 + sub < nwin && ((mu >> kl) & 1u)) {
+            uint32_t du[S::VPL], cur[S::VPL];
+            load_row8_l1(a.D + (uint64_t)u * K + kl * S::VPL, du);
+            uint32_t *dv = a.D + (uint64_t)v * K + kl * S::VPL;
+            load_row8(dv, cur);
+#pragma unroll
+            for (int q = 0; q < S::VPL; ++q) {
+              const uint32_t nd = nbr_comp<OP>(du[q], w);
+              if (nd < cur[q] && nd < atomicMin(dv + q, nd)) lowered = true;
+            }
+          }
+          // The group's first lane publishes the sectors its lanes lowered.
+          const uint32_t gbits =
+              (__ballot_sync(kFull, lowered) >> (sub * S::LPE)) & S::kSectors;
+          if (gbits && kl == 0) {
+            atomicOr(a.Mnext + v, gbits);
+            const uint32_t bit = 1u << (v & 31u);
+            if (!(atomicOr(a.chg + (v >> 5), bit) & bit)) ++n_chg;
+            any = true;
+          }
+        }
+      }
+      __syncwarp();
+    }
+  }
+  if (__any_sync(kFull, any) && lane == 0) a.ctr->update_flag = 1u;
+  n_rows = warp_sum_u64(n_rows);
+  n_edges = warp_sum_u64(n_edges);
+  n_chg = warp_sum_u64(n_chg);
+  if (lane == 0) {
+    if (n_rows) atomicAdd(&a.ctr->active, n_rows);
+    if (n_edges) atomicAdd(&a.ctr->edges, n_edges);
+    if (n_chg) atomicAdd(&a.ctr->changed, n_chg);
+  }
+}
+
+// Strategy loops start from the changed set: D = INF except D[s_k * K + k]
+// = 0, bit s_k in U and sector k / 8 of s_k in M.
+__global__ void k_seed_batch_changed(uint32_t *D, uint32_t K, const uint32_t *__restrict__ sources,
+                                     uint32_t *U, uint32_t *M) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= K) return;
+  const uint32_t s = sources[k];
+  D[(uint64_t)s * K + k] = 0u;
+  atomicOr(U + (s >> 5), 1u << (s & 31u));
+  atomicOr(M + s, 1u << (k / 8u));
 }
 
 // D = INF everywhere, D[s_k * K + k] = 0, frontier bits for every

@@ -105,8 +105,9 @@ __global__ void __launch_bounds__(kBlock) k_push_queue(push_args<OffT> a) {
 
 // ---- filtered dense pull (PULL_ALL) ------------------------------------------
 
-// Every row, in-edges from sources with a U bit only (pull_args::rd null,
-// pull_args::U the previous changed set, pull_args::chg the next one).
+// Every row (pull_args::rd null) or the frontier's rows (PULL_CHANGED), each
+// folding only in-edges from sources with a U bit (pull_args::U the
+// previous changed set, pull_args::chg the next one).
 template <int OP, typename OffT>
 __global__ void __launch_bounds__(kBlock) k_pull_all(pull_args<OffT> a) {
   if (a.ctr->done) return;

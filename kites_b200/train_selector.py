@@ -22,10 +22,17 @@ times of one source) as the ceiling.
 
 Outputs: the 1628 parameters as raw little-endian float32 (--out) and as a
 C initialiser (--inc) that the library compiles in as its default selector.
+
+--batch K trains the batched loop's selector instead (classes PLAIN, PUSH,
+PULL_ALL, PULL_CHANGED of kites_sssp_batch): the same graphs, K seeded
+sources per recorded run (kites_selector_record_batch), fitted with
+kites_selector_fit and written for selector_batch_default.inc; the held-out
+evaluation runs K-source batches of batched AUTO against batched PLAIN.
 """
 from __future__ import annotations
 
 import argparse
+import hashlib
 import json
 import os
 import sys
@@ -111,6 +118,65 @@ def collect(eng, quick: bool, per_graph: int, log):
     return np.concatenate(Xs), np.concatenate(Ts)
 
 
+def collect_batch(eng, quick: bool, k: int, runs: int, log):
+    Xs, Ts = [], []
+    for name, n, s, d, w, seed in training_graphs(quick):
+        t0 = time.time()
+        R, C, E = capi.csc_from_edges(n, s, d, w)
+        del s, d, w
+        outdeg = np.bincount(C, minlength=n)
+        cand = np.flatnonzero(outdeg > 0)
+        g = capi.Graph(eng, R, C, E)
+        rows = 0
+        cap = 8192 if name.startswith("grid") else 1024
+        for r in range(runs):
+            srcs = np.array([cand[splitmix(seed, 100 * r + j) % cand.shape[0]]
+                             for j in range(k)], dtype=np.uint32)
+            X, T = g.selector_record_batch(srcs, capi.OP_SSSP, capacity=cap)
+            Xs.append(X)
+            Ts.append(T)
+            rows += X.shape[0]
+        g.close()
+        log(f"{name}: {rows} batched iterations from {runs} runs of {k} in "
+            f"{time.time() - t0:.1f}s")
+    return np.concatenate(Xs), np.concatenate(Ts)
+
+
+def evaluate_batch(eng, scale: int, k: int, batches: int, seed: int, log):
+    n = 1 << scale
+    s, d, w = capi.gen_rmat(scale, 16 * n, 0.57, 0.19, 0.19, seed, 1, 255)
+    R, C, E = capi.csc_from_edges(n, s, d, w)
+    del s, d, w
+    outdeg = np.bincount(C, minlength=n)
+    cand = np.flatnonzero(outdeg > 0)
+    g = capi.Graph(eng, R, C, E)
+    del C, E
+    groups = [np.array([cand[splitmix(seed, 1000 * b + j) % cand.shape[0]] for j in range(k)],
+                       dtype=np.uint32) for b in range(batches)]
+    res, want = {}, {}
+    out = np.empty((n, k), np.uint32)
+    for name, strat in (("plain", capi.STRATEGY_PLAIN), ("auto", capi.STRATEGY_AUTO),
+                        ("push", capi.STRATEGY_PUSH), ("pull_all", capi.STRATEGY_PULL_ALL),
+                        ("pull_changed", capi.STRATEGY_PULL_CHANGED)):
+        o = capi.default_opts(strategy=strat)
+        g.sssp_batch(groups[0], out=out, opts=o)  # warm-up (captures the device loop)
+        total, hist = 0.0, np.zeros(capi.STRATEGY_COUNT, np.uint64)
+        for b, grp in enumerate(groups):
+            _, st = g.sssp_batch(grp, out=out, opts=o)
+            digest = hashlib.blake2b(memoryview(out).cast("B"), digest_size=16).digest()
+            if name == "plain":
+                want[b] = digest
+            elif digest != want[b]:
+                raise RuntimeError(f"batched {name} differs from batched plain on batch {b}")
+            total += st.device_ms
+            hist += np.array(st.strategy_hist[:], dtype=np.uint64)
+        res[name] = {"device_ms": total, "strategy_hist": hist.tolist()}
+        log(f"eval batched {name}: {total:.2f} ms over {batches} batches of {k}")
+    g.close()
+    res["auto_speedup_vs_plain"] = res["plain"]["device_ms"] / res["auto"]["device_ms"]
+    return res
+
+
 def evaluate(eng, scale: int, n_src: int, seed: int, log):
     n = 1 << scale
     s, d, w = capi.gen_rmat(scale, 16 * n, 0.57, 0.19, 0.19, seed, 1, 255)
@@ -167,6 +233,10 @@ def main(argv=None) -> int:
     ap.add_argument("--eval-sources", type=int, default=8)
     ap.add_argument("--eval-seed", type=int, default=99)
     ap.add_argument("--report", default=None, help="write the JSON report here")
+    ap.add_argument("--batch", type=int, default=0,
+                    help="train the batched selector with batches of this many sources")
+    ap.add_argument("--runs-per-graph", type=int, default=2)
+    ap.add_argument("--eval-batches", type=int, default=2)
     a = ap.parse_args(argv)
 
     def log(msg):
@@ -174,6 +244,29 @@ def main(argv=None) -> int:
 
     eng = capi.Engine(0)
     t0 = time.time()
+    if a.batch:
+        X, T = collect_batch(eng, a.quick, a.batch, a.runs_per_graph, log)
+        T = np.maximum(T, 1e-3)
+        log(f"dataset: {X.shape[0]} batched iterations in {time.time() - t0:.1f}s")
+        params, loss = eng.selector_fit(X, T, epochs=a.epochs, lr=a.lr, seed=1)
+        log(f"trained: loss {loss:.4f}")
+        eng.selector_load_batch(params)
+        params.astype("<f4").tofile(a.out)
+        report = {"dataset_iterations": int(X.shape[0]), "train_loss": loss, "batch": a.batch,
+                  "class_sum_ms_train": T.sum(0).tolist(),
+                  "oracle_best_over_plain_train": float(T[:, 0].sum() / T.min(1).sum())}
+        if a.eval_scale:
+            report["eval"] = evaluate_batch(eng, a.eval_scale, a.batch, a.eval_batches,
+                                            a.eval_seed, log)
+        if a.inc:
+            write_inc(params, a.inc, f"batched classes, K = {a.batch}, dataset "
+                      f"{X.shape[0]} iterations, loss {loss:.4f}")
+        log(json.dumps(report))
+        if a.report:
+            with open(a.report, "w") as f:
+                json.dump(report, f, indent=1)
+        eng.close()
+        return 0
     X, T = collect(eng, a.quick, a.sources_per_graph, log)
     T = np.maximum(T, 1e-3)
     log(f"dataset: {X.shape[0]} iterations in {time.time() - t0:.1f}s")

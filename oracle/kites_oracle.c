@@ -479,3 +479,36 @@ int kor_csc_from_edges(uint64_t n_vertices, uint64_t n_edges, const uint32_t *sr
     free(slot);
     return 0;
 }
+
+/*
+ * Exact min-label connected components of the undirected graph behind an
+ * edge list (each edge taken in both directions): union-find whose root is
+ * always the smallest id of its set, so label[v] = the smallest vertex id in
+ * v's component -- the fixed point of the min-label vertex program (init
+ * V[v] = v, nbrComp = copy, reduce = min) on the symmetrised graph, reached
+ * here without iterating.
+ */
+static uint32_t kor_root(uint32_t *parent, uint32_t x)
+{
+    while (parent[x] != x) {
+        parent[x] = parent[parent[x]];   /* path halving */
+        x = parent[x];
+    }
+    return x;
+}
+
+void kor_cc_union_find(uint64_t n_vertices, uint64_t n_edges, const uint32_t *src,
+                       const uint32_t *dst, uint32_t *label)
+{
+    for (uint64_t v = 0; v < n_vertices; ++v)
+        label[v] = (uint32_t)v;
+    for (uint64_t e = 0; e < n_edges; ++e) {
+        uint32_t a = kor_root(label, src[e]), b = kor_root(label, dst[e]);
+        if (a < b)
+            label[b] = a;
+        else if (b < a)
+            label[a] = b;
+    }
+    for (uint64_t v = 0; v < n_vertices; ++v)
+        label[v] = kor_root(label, (uint32_t)v);
+}

@@ -74,6 +74,8 @@ def lib():
                                       ctypes.c_uint32, ctypes.c_uint32, p, p, p]
         _lib.kor_csc_from_edges.restype = ctypes.c_int
         _lib.kor_csc_from_edges.argtypes = [u64, u64, p, p, p, p, p, p]
+        _lib.kor_cc_union_find.restype = None
+        _lib.kor_cc_union_find.argtypes = [u64, u64, p, p, p]
     return _lib
 
 
@@ -438,6 +440,17 @@ def certify_shortest_paths(R, C, E, dist, sources_zero, unit_weight=False):
         bad = int(np.argmax(need & ~has_tight))
         return False, f"vertex {bad} finite without a tight in-edge"
     return True, "ok"
+
+
+def cc_min_labels(n_vertices, src, dst):
+    """Exact min-label CC of the undirected graph behind an edge list (each
+    edge in both directions): the smallest vertex id of every vertex's
+    component, by union-find (kor_cc_union_find)."""
+    src = np.ascontiguousarray(src, dtype=np.uint32)
+    dst = np.ascontiguousarray(dst, dtype=np.uint32)
+    out = np.empty(n_vertices, dtype=np.uint32)
+    lib().kor_cc_union_find(n_vertices, src.shape[0], _ptr(src), _ptr(dst), _ptr(out))
+    return out
 
 
 def certify_min_label(R, C, labels):

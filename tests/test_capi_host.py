@@ -38,7 +38,7 @@ def test_exports_every_declared_symbol():
 
 
 def test_abi_version():
-    assert capi.load().kites_abi_version() == 1
+    assert capi.load().kites_abi_version() == 2
 
 
 def test_struct_layout_matches_header():

@@ -230,3 +230,24 @@ def test_live_reference_harness(has_reference, seed):
     L0 = np.arange(hg.n_vertices, dtype=np.uint32)
     np.testing.assert_array_equal(O.sanity_check(hg.R, hg.C, hg.E, L0, op=O.OP_CC_MIN)[0],
                                   _harness_csc(hg.R, hg.C, hg.E, L0, "cc"))
+
+
+def test_union_find_labels_equal_reference_cc(golden, cfg1_edges):
+    """The exact min-label oracle used at full size equals the reference's
+    own CC fixed point on config 1's symmetrised graph."""
+    s, d, _ = cfg1_edges
+    lab = O.cc_min_labels(7115, s, d)
+    want = golden["cfg1_cc"][:7115]
+    touched = np.zeros(7115, bool)
+    touched[s] = touched[d] = True
+    np.testing.assert_array_equal(lab[touched], want[touched])
+
+
+def test_union_find_labels_equal_min_label_sweep():
+    from kites_b200 import capi
+    for seed in (1, 2, 3):
+        s, d, _ = capi.gen_er(3000, 2000, seed=seed)
+        lab = O.cc_min_labels(3000, s, d)
+        R, C, _ = capi.csc_from_edges(3000, np.concatenate([s, d]), np.concatenate([d, s]))
+        want, _ = O.sanity_check(R, C, None, np.arange(3000, dtype=np.uint32), op=O.OP_CC_MIN)
+        np.testing.assert_array_equal(lab, want)
