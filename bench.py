@@ -87,6 +87,9 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-lambda", action="store_true",
+                    help="skip the kites::process user-function leg (examples/sssp_binary_csc)")
+    ap.add_argument("--lambda-sources", type=int, default=4)
     return ap.parse_args()
 
 
@@ -476,6 +479,34 @@ def run_ours(args):
         plain = {"value": reduce_over_ranks(units_per_step, world, device, "SUM") /
                  (pms * 1e-3) / 1e9, "unit": UNIT, "ms_per_step": pms}
 
+    # The drop-in API with user functions: kites::process with the reference
+    # example's four lambdas (examples/sssp_binary_csc.cu, compiled against
+    # include/kites/) on the same graph file, a few of the same sources; the
+    # last source's distances must equal the engine's (INF 2^30 - 1 there).
+    lambda_path = None
+    exe = os.path.join(ROOT, "examples", "_build", "sssp_binary_csc")
+    if rank == 0 and world == 1 and not args.no_lambda and os.path.exists(exe):
+        import tempfile
+        lsrc = [int(x) for x in srcs[:args.lambda_sources]]
+        with tempfile.TemporaryDirectory() as td:
+            dump = os.path.join(td, "V.bin")
+            r = subprocess.run([exe, cache_path(args.scale, args.edge_factor, args.seed)] +
+                               [str(x) for x in lsrc] + ["--dump", dump],
+                               capture_output=True, text=True, timeout=1200)
+            if r.returncode != 0:
+                raise RuntimeError("sssp_binary_csc failed: " + r.stderr[-500:])
+            recs = [json.loads(ln) for ln in r.stdout.splitlines() if ln.startswith("{")]
+            got = np.fromfile(dump, dtype=np.uint32)[:n]
+        ref, _ = g.sssp(lsrc[-1], out=np.empty(n, np.uint32))
+        ok = bool(np.array_equal(np.where(got == 1073741823, 0xFFFFFFFF, got), ref))
+        lms = sum(x["device_ms"] for x in recs)
+        lambda_path = {"value": sum(x["reached_edges"] for x in recs) / (lms * 1e-3) / 1e9,
+                       "unit": UNIT, "sources": len(recs), "ms_per_source": lms / len(recs),
+                       "iterations": [x["iterations"] for x in recs],
+                       "bit_exact_vs_engine": ok,
+                       "program": "examples/sssp_binary_csc.cu (kites::process, the reference "
+                                  "example's lambdas)"}
+
     # The fixed batched pull (strategy plain) on the same batches, beside a
     # batched run with another strategy.
     batched_plain = None
@@ -624,6 +655,7 @@ def run_ours(args):
             "plain": plain,
             "speedup_vs_plain": (value / plain["value"]) if plain else None,
             "batched_plain": batched_plain,
+            "lambda_path": lambda_path,
             "speedup_vs_batched_plain": (value / batched_plain["value"]) if batched_plain
             else None,
             "roofline": ({"bound": "hbm", "achieved": b_ach, "peak": peak, "unit": "GB/s",

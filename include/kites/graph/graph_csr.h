@@ -29,12 +29,22 @@
 #include <string>
 #include <vector>
 
+#include "../../kites_b200.h"
+#include "../common/cuda_error_check.cuh"
 #include "../common/globals.cuh"
 #include "../io/file_interactor.hpp"
 #include "../memory/host_pinned_buffer.cuh"
 #include "graph_base.h"
 
 namespace kites {
+
+namespace io {
+// Selects the binary CSC constructor of graph_csr (files written by
+// kites_csc_save; no counterpart in the reference, whose only on-disk form
+// of a built graph is the prepared text format).
+struct binary_csc_t {};
+constexpr binary_csc_t binary_csc{};
+}  // namespace io
 
 template <class vT, class eT, class vIdxT = unsigned int>
 class graph_csr : public graph_base {
@@ -93,6 +103,44 @@ class graph_csr : public graph_base {
     std::ifstream in;
     io::openFileToAccess(in, file);
     construct_prepared(in);
+  }
+  // A binary CSC file (kites_csc_save): R, C and E as stored, rows padded to
+  // a multiple of 128, V value-initialised and no frontier bit set -- the
+  // caller sets V and vBitmap, as a pre-processing function would, before
+  // uploading.  Directed graphs get no dir_R / dir_C here: the upload
+  // derives the out-adjacency from the CSC (vertex_per_group 1).
+  graph_csr(const std::string &file, io::binary_csc_t) : vertexPerGroup{1} {
+    static_assert(sizeof(vIdxT) == 4, "binary CSC files hold 32-bit indices");
+    uint64_t n = 0, m = 0;
+    int has_e = 0, directed = 0;
+    KITESErrorCheck(kites_csc_info(file.c_str(), &n, &m, &has_e, &directed, nullptr, 0));
+    if (m > 0xFFFFFFFFull) throw std::runtime_error("graph_csr takes < 2^32 edges");
+    std::vector<uint64_t> R64(n + 1);
+    const std::size_t n_pad = (n % 128) ? (n / 128 + 1) * 128 : n;
+    set_num_vertices(n_pad);
+    set_num_edges(m);
+    V.alloc(n_pad);
+    R.alloc(n_pad + 1);
+    C.alloc(m);
+    E.alloc(m);
+    updateFlag.alloc(1);
+    updateFlag[0] = 0;
+    std::vector<uint32_t> E32;
+    const bool direct_e = sizeof(eT) == 4;
+    if (has_e && !direct_e) E32.resize(m);
+    KITESErrorCheck(kites_csc_load(file.c_str(), R64.data(), reinterpret_cast<uint32_t *>(C.get_ptr()),
+                                   has_e ? (direct_e ? reinterpret_cast<uint32_t *>(E.get_ptr())
+                                                     : E32.data())
+                                         : nullptr));
+    for (std::size_t v = 0; v <= n_pad; ++v) R[v] = static_cast<eIdxT>(R64[v < n ? v : n]);
+    if (has_e && !direct_e)
+      for (std::size_t i = 0; i < m; ++i) E[i] = static_cast<eT>(E32[i]);
+    if (!has_e)
+      for (std::size_t i = 0; i < m; ++i) E[i] = eT();
+    for (std::size_t v = 0; v < n_pad; ++v) V[v] = vT();
+    gProp = directed ? graph_property::directed : graph_property::undirected;
+    vBitmap.alloc(n_pad);
+    vBitmap.reset();
   }
 
  private:

@@ -36,6 +36,10 @@ class graph_csr_device : public graph_base {
   device_buffer<eIdxT> dir_R;
   device_buffer<vIdxT> dir_C;
   unsigned int vertexPerGroup = 1;
+  // Device time (CUDA events around the loop) and iteration count of the
+  // last kites::process call with user functions on this graph.
+  float last_device_ms = 0.f;
+  unsigned long long last_iterations = 0;
 
   int getResidingDeviceID() const { return residing_device_id; }
   unsigned int getVertexPerGroup() const { return vertexPerGroup; }

@@ -6,6 +6,8 @@
 #ifndef KITES_B200_SANITY_CHECK_CUH_
 #define KITES_B200_SANITY_CHECK_CUH_
 
+#include <cstdio>
+#include <cstdlib>
 #include <iostream>
 
 #include "graph_csr.h"
@@ -42,6 +44,15 @@ bool sanity_check(std::size_t n, host_pinned_buffer<vT> &V, host_pinned_buffer<v
   std::cout << "### SANITY CHECK: Single CPU thread performed " << sweeps
             << " iterations in total.\n";
   host_pinned_buffer<vT> got(devV);
+  // Test harnesses that run an unmodified program name a file in
+  // KITES_SANITY_DUMP to receive the device values compared below (raw,
+  // one vT per vertex).
+  if (const char *dump = std::getenv("KITES_SANITY_DUMP")) {
+    if (std::FILE *f = std::fopen(dump, "wb")) {
+      std::fwrite(got.get_ptr(), sizeof(vT), got.size(), f);
+      std::fclose(f);
+    }
+  }
   for (std::size_t i = 0; i < got.size(); ++i)
     if (!(got[i] == V[i])) {
       std::cout << "### SANITY CHECK: MISMATCH at index " << i << "! Expected " << V[i]

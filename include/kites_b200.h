@@ -122,6 +122,14 @@ typedef struct kites_device_view {
   uint32_t *frontier[2];            /* even / odd bitmaps */
   uint32_t *update_flag;            /* one device word */
   void *stream;                     /* cudaStream_t the engine works on */
+  uint32_t *changed[2];             /* changed-row bitmaps, the frontier's size */
+  const uint32_t *chunk_rows;       /* edge-balanced chunks of the CSC: chunk k
+                                       starts at item k * chunk_items of the
+                                       sequence "row v, then its in-edges" and
+                                       chunk_rows[k] is the row holding that
+                                       item (n_chunks + 1 entries) */
+  uint64_t n_chunks;
+  uint32_t chunk_items;
 } kites_device_view;
 
 typedef struct kites_run_opts {
@@ -208,6 +216,14 @@ int kites_graph_device_view(kites_graph *g, kites_device_view *out);
 int kites_graph_get_values(kites_graph *g, void *dst, uint64_t n_vertices);
 int kites_graph_set_values(kites_graph *g, const void *src, uint64_t n_vertices);
 int kites_graph_set_frontier(kites_graph *g, const uint32_t *bits, uint64_t nbits);
+/* Enqueues on the engine's stream, without waiting, the activation step of
+ * the reference's iteration (kites/device/kernels_single_device.cuh:154-167,
+ * 288-324): for every row set in `changed` (vertex or group bits, device
+ * memory), OR the bits of its activation-adjacency targets (dir_R/dir_C, or
+ * C for undirected graphs) into `frontier`.  Allocates nothing and may be
+ * captured into a CUDA graph; the C++ front-end's process() for user
+ * functions calls it between its own pull kernels. */
+int kites_graph_activate(kites_graph *g, const uint32_t *changed, uint32_t *frontier);
 
 /* ---- runs --------------------------------------------------------------- */
 

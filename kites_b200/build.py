@@ -71,12 +71,40 @@ def build(force: bool = False, verbose: bool = False) -> str:
     return LIB
 
 
+EXAMPLES = os.path.join(ROOT, "examples")
+EXAMPLE_BIN = os.path.join(EXAMPLES, "_build")
+# Example programs over the C++ drop-in API that the tests and the benchmark
+# run (built next to the sources, in examples/_build/).
+BUILT_EXAMPLES = ["sssp_binary_csc"]
+
+
+def build_examples(force: bool = False, verbose: bool = False) -> list[str]:
+    build(force=force, verbose=verbose)
+    os.makedirs(EXAMPLE_BIN, exist_ok=True)
+    hdrs = glob.glob(os.path.join(INCLUDE, "kites", "*", "*")) + [os.path.join(INCLUDE, "kites_b200.h")]
+    out = []
+    for name in BUILT_EXAMPLES:
+        src = os.path.join(EXAMPLES, name + ".cu")
+        exe = os.path.join(EXAMPLE_BIN, name)
+        if force or _stale(exe, [src, LIB] + hdrs):
+            cmd = [NVCC] + ARCH + ["-O3", "-std=c++17", "--expt-extended-lambda", "-I", INCLUDE,
+                                   src, "-o", exe, "-L", HERE, "-lkites_b200",
+                                   "-Xlinker", "-rpath=$ORIGIN/../../kites_b200"]
+            if verbose:
+                print(" ".join(cmd), flush=True)
+            subprocess.check_call(cmd)
+        out.append(exe)
+    return out
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--force", action="store_true")
     ap.add_argument("-v", "--verbose", action="store_true")
     a = ap.parse_args(argv)
     print(build(force=a.force, verbose=a.verbose))
+    for exe in build_examples(force=a.force, verbose=a.verbose):
+        print(exe)
     return 0
 
 

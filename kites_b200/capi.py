@@ -40,7 +40,7 @@ EXPORTED = [
     "kites_graph_set_density", "kites_sssp_noalloc", "kites_graph_from_edges",
     "kites_graph_set_batch_gather", "kites_csc_save", "kites_csc_info", "kites_csc_load",
     "kites_selector_fit", "kites_selector_record_batch", "kites_selector_load_batch",
-    "kites_selector_save_batch",
+    "kites_selector_save_batch", "kites_graph_activate",
 ]
 # Selector classes of the batched loop (kites_sssp_batch with AUTO).
 BATCH_CLASS_STRATEGY = [STRATEGY_PLAIN, STRATEGY_PUSH, STRATEGY_PULL_ALL, STRATEGY_PULL_CHANGED]
@@ -72,7 +72,8 @@ class DeviceView(Structure):
         ("vertex_per_group", c_uint32), ("directed", c_int32), ("offsets64", c_int32),
         ("V", c_void_p), ("R", c_void_p), ("C", c_void_p), ("E", c_void_p),
         ("dir_R", c_void_p), ("dir_C", c_void_p), ("frontier", c_void_p * 2),
-        ("update_flag", c_void_p), ("stream", c_void_p),
+        ("update_flag", c_void_p), ("stream", c_void_p), ("changed", c_void_p * 2),
+        ("chunk_rows", c_void_p), ("n_chunks", c_uint64), ("chunk_items", c_uint32),
     ]
 
 
@@ -182,6 +183,7 @@ def load(path: str = LIB_PATH):
                                                 POINTER(c_uint32)]),
         "kites_selector_load_batch": (c_int, [vp, vp, u32]),
         "kites_selector_save_batch": (c_int, [vp, vp, u32]),
+        "kites_graph_activate": (c_int, [vp, vp, vp]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)

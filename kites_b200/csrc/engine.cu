@@ -2135,10 +2135,11 @@ extern "C" int kites_graph_upload(kites_engine *eng, const kites_csc_view *v,
                                     cudaMemcpyDefault, eng->stream);
     if (e != cudaSuccess) st = fail(KITES_ERR_CUDA, "frontier copy: %s", cudaGetErrorString(e));
   }
-  if (st == KITES_OK) st = graph_alloc(g, &p, sizeof(run_counters));
+  if (st == KITES_OK) st = graph_alloc(g, &p, 2 * sizeof(run_counters));
   if (st == KITES_OK) {
     g->ctr = (run_counters *)p;
-    cudaMemsetAsync(g->ctr, 0, sizeof(run_counters), eng->stream);
+    g->ctr_ext = g->ctr + 1;
+    cudaMemsetAsync(g->ctr, 0, 2 * sizeof(run_counters), eng->stream);
     st = graph_alloc(g, &p, 2 * KITES_MAX_RECORDED_ITERS * 8);
   }
   if (st == KITES_OK) {
@@ -2318,6 +2319,31 @@ extern "C" int kites_graph_device_view(kites_graph *g, kites_device_view *o) {
   o->frontier[1] = g->frontier[1];
   o->update_flag = &g->ctr->update_flag;
   o->stream = (void *)g->eng->stream;
+  o->changed[0] = g->changed[0];
+  o->changed[1] = g->changed[1];
+  o->chunk_rows = g->chunk_in;
+  o->n_chunks = g->nchunks_in;
+  o->chunk_items = g->chunk_items;
+  return KITES_OK;
+}
+
+extern "C" int kites_graph_activate(kites_graph *g, const uint32_t *changed, uint32_t *frontier) {
+  clear_error();
+  if (!g || !changed || !frontier) return fail(KITES_ERR_INVALID, "null argument");
+  KITES_TRY(set_device(g->eng));
+  cudaStream_t s = g->eng->stream;
+  if (g->off64) {
+    chunk_geom<uint64_t> ga{(const uint64_t *)g->dirR, g->dirC, g->chunk_dir, g->nchunks_dir,
+                            g->n_dir_rows, g->n_dir_rows + g->n_dir_edges, g->chunk_items};
+    expand_args<uint64_t> ea{ga, changed, frontier, g->ctr_ext, 0u, 0u, 0ull};
+    k_expand_chunked<uint64_t><<<g->expand_grid, kBlock, 0, s>>>(ea);
+  } else {
+    chunk_geom<uint32_t> ga{(const uint32_t *)g->dirR, g->dirC, g->chunk_dir, g->nchunks_dir,
+                            g->n_dir_rows, g->n_dir_rows + g->n_dir_edges, g->chunk_items};
+    expand_args<uint32_t> ea{ga, changed, frontier, g->ctr_ext, 0u, 0u, 0ull};
+    k_expand_chunked<uint32_t><<<g->expand_grid, kBlock, 0, s>>>(ea);
+  }
+  KITES_CUDA_TRY(cudaGetLastError());
   return KITES_OK;
 }
 

@@ -81,6 +81,7 @@ struct kites_graph {
   uint32_t *changed[2] = {nullptr, nullptr};
 
   kites_internal::run_counters *ctr = nullptr;
+  kites_internal::run_counters *ctr_ext = nullptr;  // kites_graph_activate's (never done)
   unsigned long long *rec_active = nullptr;
   unsigned long long *rec_edges = nullptr;
 

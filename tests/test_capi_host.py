@@ -51,7 +51,7 @@ int main(void) {
   printf("csc %zu\nview %zu\nopts %zu\nstats %zu\n", sizeof(kites_csc_view),
          sizeof(kites_device_view), sizeof(kites_run_opts), sizeof(kites_run_stats));
   P(kites_csc_view, on_device) P(kites_csc_view, frontier_nbits)
-  P(kites_device_view, stream) P(kites_run_opts, time_kernels)
+  P(kites_device_view, stream) P(kites_device_view, chunk_items) P(kites_run_opts, time_kernels)
   P(kites_run_stats, pull_kernel_bytes) P(kites_run_stats, iter_edges)
   P(kites_run_stats, pull_dense_bytes) P(kites_csc_view, offsets64)
   return 0;
@@ -71,6 +71,7 @@ int main(void) {
     assert int(got["kites_csc_view.on_device"]) == capi.CscView.on_device.offset
     assert int(got["kites_csc_view.frontier_nbits"]) == capi.CscView.frontier_nbits.offset
     assert int(got["kites_device_view.stream"]) == capi.DeviceView.stream.offset
+    assert int(got["kites_device_view.chunk_items"]) == capi.DeviceView.chunk_items.offset
     assert int(got["kites_run_opts.time_kernels"]) == capi.RunOpts.time_kernels.offset
     assert int(got["kites_run_stats.pull_kernel_bytes"]) == capi.RunStats.pull_kernel_bytes.offset
     assert int(got["kites_run_stats.iter_edges"]) == capi.RunStats.iter_edges.offset
