@@ -185,7 +185,12 @@ int kites_engine_destroy(kites_engine *eng);
 /* Replaces nv_gpu::queryMemUsage (nv_gpu.cuh:78-86), in bytes. */
 int kites_engine_mem_usage(kites_engine *eng, uint64_t *used, uint64_t *total,
                            uint64_t *pool_reserved);
-int kites_engine_sync(kites_engine *eng);  /* nv_gpu::sync (nv_gpu.cuh:45-48) */
+/* nv_gpu::sync (nv_gpu.cuh:45-48): waits for the engine stream and for the
+ * copies of kites_sssp_batch_async. */
+int kites_engine_sync(kites_engine *eng);
+/* Orders the engine stream after every copy kites_sssp_batch_async has
+ * issued so far, without blocking the host (no reference counterpart). */
+int kites_engine_join(kites_engine *eng);
 /* The cudaStream_t every engine call is ordered on; replaces
  * nv_gpu::getSsEven (nv_gpu.cuh:56-58), the reference's working stream. */
 int kites_engine_stream(kites_engine *eng, void **stream_out);
@@ -250,6 +255,17 @@ int kites_sssp(kites_engine *eng, kites_graph *g, int op, uint32_t source,
 int kites_sssp_batch(kites_engine *eng, kites_graph *g, int op,
                      const uint32_t *sources, uint32_t k, uint32_t *dist_out,
                      const kites_run_opts *opts, kites_run_stats *stats);
+
+/* The same, returning as soon as the distances are computed: they are
+ * copied on the device into a per-graph staging buffer (n x K values, kept
+ * by the graph) and from there to dist_out on a second stream, so the next
+ * batch computes while this one's result crosses to the host (give pinned
+ * host memory for the copy to overlap).  dist_out must not be read before
+ * kites_engine_sync (or, on the device side, kites_engine_join) and must
+ * stay valid until then.  No reference counterpart. */
+int kites_sssp_batch_async(kites_engine *eng, kites_graph *g, int op,
+                           const uint32_t *sources, uint32_t k, uint32_t *dist_out,
+                           const kites_run_opts *opts, kites_run_stats *stats);
 
 /* Multi-seed SSSP/BFS: every seed starts at 0 (one super-source).  On a
  * disjoint union of graphs with one seed per member this runs a whole batch

@@ -40,7 +40,8 @@ EXPORTED = [
     "kites_graph_set_density", "kites_sssp_noalloc", "kites_graph_from_edges",
     "kites_graph_set_batch_gather", "kites_csc_save", "kites_csc_info", "kites_csc_load",
     "kites_selector_fit", "kites_selector_record_batch", "kites_selector_load_batch",
-    "kites_selector_save_batch", "kites_graph_activate",
+    "kites_selector_save_batch", "kites_graph_activate", "kites_sssp_batch_async",
+    "kites_engine_join",
 ]
 # Selector classes of the batched loop (kites_sssp_batch with AUTO).
 BATCH_CLASS_STRATEGY = [STRATEGY_PLAIN, STRATEGY_PUSH, STRATEGY_PULL_ALL, STRATEGY_PULL_CHANGED]
@@ -184,6 +185,9 @@ def load(path: str = LIB_PATH):
         "kites_selector_load_batch": (c_int, [vp, vp, u32]),
         "kites_selector_save_batch": (c_int, [vp, vp, u32]),
         "kites_graph_activate": (c_int, [vp, vp, vp]),
+        "kites_sssp_batch_async": (c_int, [vp, vp, c_int, vp, u32, vp, POINTER(RunOpts),
+                                           POINTER(RunStats)]),
+        "kites_engine_join": (c_int, [vp]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)

@@ -1318,6 +1318,40 @@ int prepare_batch(kites_graph *g, uint32_t K, uint32_t items, batch_state *b) {
   return KITES_OK;
 }
 
+// Copies a batch result (n_given x K values of D) to dist_out.  Synchronous,
+// or -- for kites_sssp_batch_async -- staged: D is copied on the device into
+// the graph's staging buffer (after the previous staged result has left it)
+// and copy_stream moves the staging buffer to dist_out while the engine
+// stream is free for the next batch.
+int deliver_batch(kites_graph *g, const uint32_t *D, uint32_t *dist_out, uint64_t values,
+                  bool async) {
+  kites_engine *eng = g->eng;
+  cudaStream_t s = eng->stream;
+  if (!async) {
+    KITES_CUDA_TRY(cudaMemcpyAsync(dist_out, D, values * 4, cudaMemcpyDefault, s));
+    KITES_CUDA_TRY(cudaStreamSynchronize(s));
+    return KITES_OK;
+  }
+  if (g->stage_cap < values) {
+    KITES_CUDA_TRY(cudaStreamWaitEvent(s, eng->copied, 0));
+    graph_release(g, g->stage);
+    g->stage = nullptr;
+    g->stage_cap = 0;
+    void *p;
+    KITES_TRY(graph_alloc(g, &p, values * 4));
+    g->stage = (uint32_t *)p;
+    g->stage_cap = values;
+  }
+  KITES_CUDA_TRY(cudaStreamWaitEvent(s, eng->copied, 0));
+  KITES_CUDA_TRY(cudaMemcpyAsync(g->stage, D, values * 4, cudaMemcpyDeviceToDevice, s));
+  KITES_CUDA_TRY(cudaEventRecord(eng->staged, s));
+  KITES_CUDA_TRY(cudaStreamWaitEvent(eng->copy_stream, eng->staged, 0));
+  KITES_CUDA_TRY(cudaMemcpyAsync(dist_out, g->stage, values * 4, cudaMemcpyDefault,
+                                 eng->copy_stream));
+  KITES_CUDA_TRY(cudaEventRecord(eng->copied, eng->copy_stream));
+  return KITES_OK;
+}
+
 template <int OP, typename OffT, int K>
 int run_batch(kites_graph *g, const uint32_t *sources, uint32_t *dist_out,
               const kites_run_opts &o, kites_run_stats *st) {
@@ -1361,10 +1395,7 @@ int run_batch(kites_graph *g, const uint32_t *sources, uint32_t *dist_out,
     return launch_batch_iteration<OP, OffT, K>(g, b, parity, h, hh, l, tp);
   };
   KITES_TRY(drive_loop(g, o, loop_key{OP, 1000 + (int)K}, launch, &c, &ms, &launches, st));
-  if (dist_out) {
-    KITES_CUDA_TRY(cudaMemcpyAsync(dist_out, b.D, g->n_given * K * 4, cudaMemcpyDefault, s));
-    KITES_CUDA_TRY(cudaStreamSynchronize(s));
-  }
+  if (dist_out) KITES_TRY(deliver_batch(g, b.D, dist_out, g->n_given * K, g->async_out));
   if (st) {
     st->iterations = c.iterations;
     st->device_ms = ms;
@@ -1733,10 +1764,7 @@ int run_batch_flex(kites_graph *g, const uint32_t *sources, uint32_t *dist_out,
     KITES_TRY(drive_loop(g, o, loop_key{OP, 2000 + 16 * strategy + (int)(K / 16)}, launch, &c,
                          &ms, &launches, st));
   }
-  if (dist_out) {
-    KITES_CUDA_TRY(cudaMemcpyAsync(dist_out, f.D, g->n_given * K * 4, cudaMemcpyDefault, s));
-    KITES_CUDA_TRY(cudaStreamSynchronize(s));
-  }
+  if (dist_out) KITES_TRY(deliver_batch(g, f.D, dist_out, g->n_given * K, g->async_out));
   if (st) {
     st->iterations = c.iterations;
     st->device_ms = ms;
@@ -1956,7 +1984,11 @@ extern "C" int kites_engine_create(int device, kites_engine **out) {
         (ce = cudaEventCreate(&eng->ev0)) != cudaSuccess ||
         (ce = cudaEventCreate(&eng->ev1)) != cudaSuccess ||
         (ce = cudaEventCreate(&eng->kev0)) != cudaSuccess ||
-        (ce = cudaEventCreate(&eng->kev1)) != cudaSuccess) {
+        (ce = cudaEventCreate(&eng->kev1)) != cudaSuccess ||
+        (ce = cudaStreamCreateWithFlags(&eng->copy_stream, cudaStreamNonBlocking)) !=
+            cudaSuccess ||
+        (ce = cudaEventCreateWithFlags(&eng->staged, cudaEventDisableTiming)) != cudaSuccess ||
+        (ce = cudaEventCreateWithFlags(&eng->copied, cudaEventDisableTiming)) != cudaSuccess) {
       st = fail(KITES_ERR_CUDA, "stream/event creation failed: %s", cudaGetErrorString(ce));
       break;
     }
@@ -2020,6 +2052,7 @@ extern "C" int kites_engine_destroy(kites_engine *eng) {
   if (!eng) return KITES_OK;
   cudaSetDevice(eng->device);
   if (eng->stream) cudaStreamSynchronize(eng->stream);
+  if (eng->copy_stream) cudaStreamSynchronize(eng->copy_stream);
   // Graphs die with their engine; their handles are invalid afterwards.
   while (!eng->graphs.empty()) kites_graph_destroy(eng->graphs.back());
   if (eng->pinned) cudaFreeHost(eng->pinned);
@@ -2029,6 +2062,9 @@ extern "C" int kites_engine_destroy(kites_engine *eng) {
   if (eng->ev1) cudaEventDestroy(eng->ev1);
   if (eng->kev0) cudaEventDestroy(eng->kev0);
   if (eng->kev1) cudaEventDestroy(eng->kev1);
+  if (eng->staged) cudaEventDestroy(eng->staged);
+  if (eng->copied) cudaEventDestroy(eng->copied);
+  if (eng->copy_stream) cudaStreamDestroy(eng->copy_stream);
   if (eng->stream) cudaStreamDestroy(eng->stream);
   if (eng->pool) cudaMemPoolDestroy(eng->pool);
   delete eng;
@@ -2064,12 +2100,23 @@ extern "C" int kites_engine_sync(kites_engine *eng) {
   if (!eng) return fail(KITES_ERR_INVALID, "null engine");
   KITES_TRY(set_device(eng));
   KITES_CUDA_TRY(cudaStreamSynchronize(eng->stream));
+  KITES_CUDA_TRY(cudaStreamSynchronize(eng->copy_stream));
+  return KITES_OK;
+}
+
+extern "C" int kites_engine_join(kites_engine *eng) {
+  clear_error();
+  if (!eng) return fail(KITES_ERR_INVALID, "null engine");
+  KITES_TRY(set_device(eng));
+  KITES_CUDA_TRY(cudaEventRecord(eng->copied, eng->copy_stream));
+  KITES_CUDA_TRY(cudaStreamWaitEvent(eng->stream, eng->copied, 0));
   return KITES_OK;
 }
 
 extern "C" int kites_graph_destroy(kites_graph *g) {
   if (!g) return KITES_OK;
   cudaSetDevice(g->eng->device);
+  cudaStreamSynchronize(g->eng->copy_stream);
   cudaStreamSynchronize(g->eng->stream);
   for (auto &kv : g->loops) {
     cudaGraphExecDestroy(kv.second.second);
@@ -2507,11 +2554,33 @@ extern "C" int kites_pagerank(kites_engine *eng, kites_graph *g, uint64_t n_real
                   : run_pagerank<uint32_t>(g, n_real, rank_out, o, stats);
 }
 
+static int sssp_batch(kites_engine *eng, kites_graph *g, int op, const uint32_t *sources,
+                      uint32_t k, uint32_t *dist_out, const kites_run_opts *opts,
+                      kites_run_stats *stats);
+
 extern "C" int kites_sssp_batch(kites_engine *eng, kites_graph *g, int op,
                                 const uint32_t *sources, uint32_t k, uint32_t *dist_out,
                                 const kites_run_opts *opts, kites_run_stats *stats) {
   clear_error();
   KITES_TRY(check_graph(eng, g));
+  g->async_out = false;
+  return sssp_batch(eng, g, op, sources, k, dist_out, opts, stats);
+}
+
+extern "C" int kites_sssp_batch_async(kites_engine *eng, kites_graph *g, int op,
+                                      const uint32_t *sources, uint32_t k, uint32_t *dist_out,
+                                      const kites_run_opts *opts, kites_run_stats *stats) {
+  clear_error();
+  KITES_TRY(check_graph(eng, g));
+  g->async_out = true;
+  const int st = sssp_batch(eng, g, op, sources, k, dist_out, opts, stats);
+  g->async_out = false;
+  return st;
+}
+
+static int sssp_batch(kites_engine *eng, kites_graph *g, int op, const uint32_t *sources,
+                      uint32_t k, uint32_t *dist_out, const kites_run_opts *opts,
+                      kites_run_stats *stats) {
   if (!sources) return fail(KITES_ERR_INVALID, "null sources");
   if (g->esize != 4 && op != OP_BFS) return fail(KITES_ERR_UNSUPPORTED, "SSSP needs 4-byte edge values");
   if (k != 16 && k != 32 && k != 64 && k != 128 && k != 256)

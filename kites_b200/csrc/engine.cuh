@@ -14,6 +14,10 @@ struct kites_engine {
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   cudaEvent_t kev0 = nullptr, kev1 = nullptr;   // per-kernel timing
+  // Asynchronous batch results: device-to-host copies run on copy_stream
+  // (staged = the staging buffer holds a result, copied = its copy is done).
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t staged = nullptr, copied = nullptr;
   cudaMemPool_t pool = nullptr;   // stream-ordered pool owning every buffer
   int sm_count = 0;
   int l2_bytes = 0;
@@ -88,6 +92,9 @@ struct kites_graph {
   // Batched multi-source runs (V x K distances), allocated on first use.
   uint32_t *batchD = nullptr;
   uint64_t batch_cap = 0;            // elements of batchD
+  uint32_t *stage = nullptr;         // kites_sssp_batch_async: the last result, for copy_stream
+  uint64_t stage_cap = 0;
+  bool async_out = false;            // the running batch call delivers through stage
   uint32_t *bbits = nullptr;         // vertex-level [f0|c0|f1|c1] when vpg > 1
   uint64_t bnwords = 0;
   uint32_t batch_chunk_items = 0;    // chunk size chunk_batch was built with

@@ -182,10 +182,16 @@ __global__ void __launch_bounds__(kBlock, K >= 256 ? 2 : 4)
               const uint32_t j = jj + r * S::EPW + sub;
               const uint32_t src = kMasked ? (j < ntile ? (uint32_t)s_slot[wib][j] : 0u)
                                            : (j & 31u);
+              // Every lane takes part in every shuffle (full mask), whether
+              // or not its slot gathers anything.
               const uint32_t u = __shfl_sync(kFull, cC, src);
               wq[r] = __shfl_sync(kFull, cE, src);
-              bool take = j < ntile;
-              if constexpr (kMasked) take = take && ((__shfl_sync(kFull, cM, src) >> kl) & 1u);
+              const uint32_t mu = kMasked ? __shfl_sync(kFull, cM, src) : kFull;
+              bool take = j < ntile && ((mu >> kl) & 1u);
+              if (kMasked && take && u >= a.g.n_rows) {  // never index with an id out of range
+                raise_error(a.ctr, kErrIndex);
+                take = false;
+              }
               if (take) {
                 load_row8(a.D + (uint64_t)u * K + kl * S::VPL, row[r]);
               } else {

@@ -168,3 +168,26 @@ def test_batched_strategies_on_64bit_offsets(engine, uploaded, strategy):
         np.testing.assert_array_equal(got, plain)
     finally:
         g64.close()
+
+
+@pytest.mark.parametrize("strategy", [capi.STRATEGY_PLAIN, capi.STRATEGY_AUTO])
+def test_async_batches_deliver_every_result(engine, uploaded, strategy):
+    """kites_sssp_batch_async: three batches issued back to back, each into
+    its own pinned buffer, equal the synchronous results once the engine is
+    synchronised (the copies run on the second stream)."""
+    import ctypes
+
+    import torch
+
+    g, R, C, E, n = uploaded["rmat14"]
+    lib = capi.load()
+    o = capi.default_opts(strategy=strategy)
+    groups = [sources_for(n, 64, 40 + i) for i in range(3)]
+    want = [g.sssp_batch(grp)[0] for grp in groups]
+    bufs = [torch.empty((n, 64), dtype=torch.int32, pin_memory=True) for _ in groups]
+    for grp, buf in zip(groups, bufs):
+        capi._check(lib.kites_sssp_batch_async(engine._h, g._h, capi.OP_SSSP, capi._p(grp), 64,
+                                               capi._p(buf), ctypes.byref(o), None))
+    engine.sync()
+    for w, buf in zip(want, bufs):
+        np.testing.assert_array_equal(buf.numpy().view(np.uint32), w)

@@ -64,7 +64,7 @@ def test_cfg1_cc_golden(engine, golden, cfg1_edges):
     np.testing.assert_array_equal(labels, golden["cfg1_cc"][:7115])
 
 
-@pytest.mark.parametrize("vpg", [1, 2, 4, 8, 32, 64])
+@pytest.mark.parametrize("vpg", [1, 2, 4, 8, 16, 32, 64])
 def test_reference_process_semantics_vpg(engine, cfg1_edges, vpg):
     """kites::process on a host graph built with the reference's rules
     (example pre-processing, INF 2^30-1, wrap-around add) for every vpg."""

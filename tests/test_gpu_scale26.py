@@ -87,7 +87,7 @@ def test_scale26_cc_symmetrised(rmat26, engine):
     gs = capi.Graph.from_edges(engine, n, np.concatenate([s, d]), np.concatenate([d, s]),
                                directed=False)
     try:
-        assert gs.n_edges == 2 * s.shape[0] > (1 << 31)
+        assert gs.n_edges == 2 * s.shape[0] == 1 << 31  # past the old 2^31 - 1 limit
         labels, st = gs.cc()
         np.testing.assert_array_equal(labels, want)
         assert st.iterations > 1
