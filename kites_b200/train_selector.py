@@ -57,7 +57,31 @@ def uniform(seed: int, k: int, lo: float, hi: float) -> float:
     return lo + (hi - lo) * (splitmix(seed, k) >> 11) / float(1 << 53)
 
 
-def training_graphs(quick: bool):
+def config3_specs(n_graphs: int = 200):
+    """The selector training set of the benchmark configuration: n_graphs
+    seeded graphs, four in five R-MAT (scale uniform in 16..22, edge factor
+    16, (a, b, c) uniform within +-0.04 of (0.57, 0.19, 0.19), scaled down to
+    a sum of 0.99 where they pass it), one in five a 2-D grid road-like graph
+    (side log-uniform in 1024..4096, 4-neighbour, weights U[1, 1000])."""
+    specs = []
+    for i in range(n_graphs):
+        seed = 5000 + i
+        if i % 5 == 4:
+            side = int(round(1024 * 4 ** uniform(seed, 0, 0.0, 1.0)))
+            specs.append(("grid", side, 4, 0, 0, 0, seed))
+            continue
+        sc = 16 + int(uniform(seed, 0, 0, 7))
+        a = uniform(seed, 1, 0.53, 0.61)
+        b = uniform(seed, 2, 0.15, 0.23)
+        c = uniform(seed, 3, 0.15, 0.23)
+        if a + b + c > 0.99:
+            f = 0.99 / (a + b + c)
+            a, b, c = a * f, b * f, c * f
+        specs.append(("rmat", sc, 16, a, b, c, seed))
+    return specs
+
+
+def training_graphs(quick: bool, config3: int = 0):
     """(name, n, src, dst, w) tuples, generated one at a time."""
     specs = []
     scales = [16, 17, 18, 19, 20, 21, 22] if not quick else [16, 18, 20]
@@ -76,6 +100,8 @@ def training_graphs(quick: bool):
         specs.append(("er", lv, int(uniform(seed, 0, 4, 16)), 0, 0, 0, seed))
     for i, side in enumerate([256, 512, 1024, 1536] if not quick else [256, 768]):
         specs.append(("grid", side, 4, 0, 0, 0, 3000 + i))
+    if config3:
+        specs = config3_specs(config3)
     for kind, p, ef, a, b, c, seed in specs:
         if kind == "rmat":
             n = 1 << p
@@ -98,16 +124,16 @@ def pick_sources(src, n, count, seed):
     return [int(cand[splitmix(seed, 7 + k) % cand.shape[0]]) for k in range(count)]
 
 
-def collect(eng, quick: bool, per_graph: int, log):
+def collect(eng, quick: bool, per_graph: int, log, config3: int = 0):
     Xs, Ts = [], []
-    for name, n, s, d, w, seed in training_graphs(quick):
+    for name, n, s, d, w, seed in training_graphs(quick, config3):
         t0 = time.time()
         R, C, E = capi.csc_from_edges(n, s, d, w)
         srcs = pick_sources(s, n, per_graph, seed)
         del s, d, w
         g = capi.Graph(eng, R, C, E)
         rows = 0
-        cap = 8192 if name.startswith("grid") else 1024
+        cap = 32768 if name.startswith("grid") else 1024
         for src in srcs:
             X, T = g.selector_record(capi.OP_SSSP, src, capacity=cap)
             Xs.append(X)
@@ -118,9 +144,9 @@ def collect(eng, quick: bool, per_graph: int, log):
     return np.concatenate(Xs), np.concatenate(Ts)
 
 
-def collect_batch(eng, quick: bool, k: int, runs: int, log):
+def collect_batch(eng, quick: bool, k: int, runs: int, log, config3: int = 0):
     Xs, Ts = [], []
-    for name, n, s, d, w, seed in training_graphs(quick):
+    for name, n, s, d, w, seed in training_graphs(quick, config3):
         t0 = time.time()
         R, C, E = capi.csc_from_edges(n, s, d, w)
         del s, d, w
@@ -128,7 +154,7 @@ def collect_batch(eng, quick: bool, k: int, runs: int, log):
         cand = np.flatnonzero(outdeg > 0)
         g = capi.Graph(eng, R, C, E)
         rows = 0
-        cap = 8192 if name.startswith("grid") else 1024
+        cap = 32768 if name.startswith("grid") else 1024
         for r in range(runs):
             srcs = np.array([cand[splitmix(seed, 100 * r + j) % cand.shape[0]]
                              for j in range(k)], dtype=np.uint32)
@@ -236,6 +262,9 @@ def main(argv=None) -> int:
     ap.add_argument("--batch", type=int, default=0,
                     help="train the batched selector with batches of this many sources")
     ap.add_argument("--runs-per-graph", type=int, default=2)
+    ap.add_argument("--config3", type=int, default=0,
+                    help="train on this many graphs of the configuration's recipe "
+                         "(R-MAT 16-22 with jittered a,b,c and grids of side 1024-4096)")
     ap.add_argument("--eval-batches", type=int, default=2)
     a = ap.parse_args(argv)
 
@@ -245,7 +274,7 @@ def main(argv=None) -> int:
     eng = capi.Engine(0)
     t0 = time.time()
     if a.batch:
-        X, T = collect_batch(eng, a.quick, a.batch, a.runs_per_graph, log)
+        X, T = collect_batch(eng, a.quick, a.batch, a.runs_per_graph, log, a.config3)
         T = np.maximum(T, 1e-3)
         log(f"dataset: {X.shape[0]} batched iterations in {time.time() - t0:.1f}s")
         params, loss = eng.selector_fit(X, T, epochs=a.epochs, lr=a.lr, seed=1)
@@ -267,7 +296,7 @@ def main(argv=None) -> int:
                 json.dump(report, f, indent=1)
         eng.close()
         return 0
-    X, T = collect(eng, a.quick, a.sources_per_graph, log)
+    X, T = collect(eng, a.quick, a.sources_per_graph, log, a.config3)
     T = np.maximum(T, 1e-3)
     log(f"dataset: {X.shape[0]} iterations in {time.time() - t0:.1f}s")
     params, loss = eng.selector_train(X, T, epochs=a.epochs, lr=a.lr, seed=1)
