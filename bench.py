@@ -56,7 +56,7 @@ UNIT = "GTEPS"
 REF_LIB = os.path.join(ROOT, "oracle", "_ref", "libref_harness.so")
 # kites_run_opts.strategy values (include/kites_b200.h).
 STRATEGIES = {"plain": 0, "auto": 1, "push": 2, "pull_all": 3, "tpv1": 4, "tpv4": 5,
-              "tpv8": 6, "tpv32": 7}
+              "tpv8": 6, "tpv32": 7, "pull_changed": 8}
 
 
 def parse():
@@ -72,9 +72,11 @@ def parse():
     ap.add_argument("--mode", default="batch", choices=["batch", "single"],
                     help="batch: --batch sources per pass over the edges (headline); "
                          "single: one source at a time through kites_sssp")
-    ap.add_argument("--strategy", default="plain", choices=sorted(STRATEGIES),
-                    help="per-iteration strategy: auto = the learned selector; batch mode "
-                         "takes plain, auto, push, pull_all and pull_changed")
+    ap.add_argument("--strategy", default=None, choices=sorted(STRATEGIES),
+                    help="per-iteration strategy: auto = the learned selector (the default of "
+                         "--mode batch: learned + batched); plain = the fixed plain kernel (the "
+                         "default of --mode single); batch mode takes plain, auto, push, "
+                         "pull_all and pull_changed")
     ap.add_argument("--batch-gather", default="loads", choices=["loads", "tma"],
                     help="how the batched pull fetches source rows: register loads or "
                          "TMA tile::gather4 copies")
@@ -96,7 +98,10 @@ def parse():
     ap.add_argument("--batch-selector", default=None,
                     help="load the batched selector's weights from this file (1628 float32) "
                          "instead of the compiled-in default")
-    return ap.parse_args()
+    a = ap.parse_args()
+    if a.strategy is None:
+        a.strategy = "auto" if a.mode == "batch" else "plain"
+    return a
 
 
 # ---------------------------------------------------------------------------
@@ -615,9 +620,22 @@ def run_ours(args):
         e1.record(stream)
         torch.cuda.synchronize()
         e_ms = reduce_over_ranks(e0.elapsed_time(e1), world, device, "MAX")
+        # The same device-to-host copy alone, for scale: the pipeline is bound
+        # by it whenever it takes longer than a batch's compute.
+        src_dev = torch.empty((n, K), dtype=torch.int32, device=device)
+        torch.cuda.synchronize()
+        c0 = torch.cuda.Event(enable_timing=True)
+        c1 = torch.cuda.Event(enable_timing=True)
+        c0.record()
+        pinned.copy_(src_dev, non_blocking=True)
+        c1.record()
+        torch.cuda.synchronize()
+        d2h_gbs = 4.0 * n * K / (c0.elapsed_time(c1) * 1e-3) / 1e9
+        del src_dev
         e2e = {"value": total_units / (e_ms * 1e-3) / 1e9, "unit": UNIT,
                "h2d_bytes_per_step": 4 * len(srcs),
-               "d2h_bytes_per_step": 4 * n * len(srcs)}
+               "d2h_bytes_per_step": 4 * n * len(srcs),
+               "d2h_gbs_alone": d2h_gbs}
 
     # Correctness of what was timed, after the timed region: the distances of
     # the first batch (or the first sources of --mode single), column for

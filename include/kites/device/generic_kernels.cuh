@@ -84,39 +84,51 @@ __device__ __forceinline__ void fold_runs(vT &x, uint32_t lane, uint32_t end, FR
 // Folds nbrCompF over the in-edges of the warp's rows: lane j's row has
 // cnt[j] edges starting at beg[j] (ex = exclusive prefix of the counts,
 // total = their sum); the fold of row j lands in acc[j], has[j] says whether
-// it holds any value (rows with no edges hold none).
+// it holds any value (rows with no edges hold none).  kUnroll windows of 32
+// edges have their values (the V[C[e]] gathers) in flight before any is
+// reduced.
+constexpr int kUnroll = 4;
+
 template <class vT, class eT, class OffT, class FComp, class FRed>
 __device__ __forceinline__ void fold_edges(uint32_t lane, uint32_t total, const uint32_t *ex,
                                            const OffT *beg, const uint32_t *__restrict__ C,
                                            const vT *V, eT *E, vT *acc, uint8_t *has,
                                            FComp &fComp, FRed &fRed) {
-  for (uint32_t base = 0; base < total; base += 32) {
-    const uint32_t i = base + lane;
-    uint32_t owner = 32u;
-    vT part{};
-    if (i < total) {
-      uint32_t j = 0;
+  for (uint32_t base = 0; base < total; base += 32 * kUnroll) {
+    uint32_t owner[kUnroll];
+    vT part[kUnroll];
 #pragma unroll
-      for (uint32_t step = 16; step; step >>= 1)
-        if (ex[j + step] <= i) j += step;
-      owner = j;
-      const OffT e = beg[j] + (OffT)(i - ex[j]);
-      const vT src = V[C[e]];
-      fComp(part, src, E + e);
-    }
-    uint32_t s, t;
-    bool head;
-    run_bounds(owner, lane, &s, &t, &head);
-    fold_runs(part, lane, t, fRed);
-    if (head && owner < 32u) {
-      if (has[owner]) {
-        fRed(acc[owner], part);
-      } else {
-        acc[owner] = part;
-        has[owner] = 1;
+    for (int u = 0; u < kUnroll; ++u) {
+      const uint32_t i = base + u * 32 + lane;
+      owner[u] = 32u;
+      part[u] = vT{};
+      if (i < total) {
+        uint32_t j = 0;
+#pragma unroll
+        for (uint32_t step = 16; step; step >>= 1)
+          if (ex[j + step] <= i) j += step;
+        owner[u] = j;
+        const OffT e = beg[j] + (OffT)(i - ex[j]);
+        const vT src = V[C[e]];
+        fComp(part[u], src, E + e);
       }
     }
-    __syncwarp();
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) {
+      uint32_t s, t;
+      bool head;
+      run_bounds(owner[u], lane, &s, &t, &head);
+      fold_runs(part[u], lane, t, fRed);
+      if (head && owner[u] < 32u) {
+        if (has[owner[u]]) {
+          fRed(acc[owner[u]], part[u]);
+        } else {
+          acc[owner[u]] = part[u];
+          has[owner[u]] = 1;
+        }
+      }
+      __syncwarp();
+    }
   }
 }
 

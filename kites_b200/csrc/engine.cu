@@ -1335,6 +1335,7 @@ int deliver_batch(kites_graph *g, const uint32_t *D, uint32_t *dist_out, uint64_
   }
   if (g->stage_cap < values) {
     KITES_CUDA_TRY(cudaStreamWaitEvent(s, eng->copied, 0));
+    KITES_CUDA_TRY(cudaStreamWaitEvent(s, eng->copied2, 0));
     graph_release(g, g->stage);
     g->stage = nullptr;
     g->stage_cap = 0;
@@ -1344,12 +1345,20 @@ int deliver_batch(kites_graph *g, const uint32_t *D, uint32_t *dist_out, uint64_
     g->stage_cap = values;
   }
   KITES_CUDA_TRY(cudaStreamWaitEvent(s, eng->copied, 0));
+  KITES_CUDA_TRY(cudaStreamWaitEvent(s, eng->copied2, 0));
   KITES_CUDA_TRY(cudaMemcpyAsync(g->stage, D, values * 4, cudaMemcpyDeviceToDevice, s));
   KITES_CUDA_TRY(cudaEventRecord(eng->staged, s));
+  // Two halves on two streams, so that two copy engines share the transfer.
+  const uint64_t half = (values / 2 + 7) / 8 * 8;
   KITES_CUDA_TRY(cudaStreamWaitEvent(eng->copy_stream, eng->staged, 0));
-  KITES_CUDA_TRY(cudaMemcpyAsync(dist_out, g->stage, values * 4, cudaMemcpyDefault,
-                                 eng->copy_stream));
+  KITES_CUDA_TRY(cudaMemcpyAsync(dist_out, g->stage, std::min(half, values) * 4,
+                                 cudaMemcpyDefault, eng->copy_stream));
   KITES_CUDA_TRY(cudaEventRecord(eng->copied, eng->copy_stream));
+  KITES_CUDA_TRY(cudaStreamWaitEvent(eng->copy_stream2, eng->staged, 0));
+  if (values > half)
+    KITES_CUDA_TRY(cudaMemcpyAsync(dist_out + half, g->stage + half, (values - half) * 4,
+                                   cudaMemcpyDefault, eng->copy_stream2));
+  KITES_CUDA_TRY(cudaEventRecord(eng->copied2, eng->copy_stream2));
   return KITES_OK;
 }
 
@@ -1988,8 +1997,11 @@ extern "C" int kites_engine_create(int device, kites_engine **out) {
         (ce = cudaEventCreate(&eng->kev1)) != cudaSuccess ||
         (ce = cudaStreamCreateWithFlags(&eng->copy_stream, cudaStreamNonBlocking)) !=
             cudaSuccess ||
+        (ce = cudaStreamCreateWithFlags(&eng->copy_stream2, cudaStreamNonBlocking)) !=
+            cudaSuccess ||
         (ce = cudaEventCreateWithFlags(&eng->staged, cudaEventDisableTiming)) != cudaSuccess ||
-        (ce = cudaEventCreateWithFlags(&eng->copied, cudaEventDisableTiming)) != cudaSuccess) {
+        (ce = cudaEventCreateWithFlags(&eng->copied, cudaEventDisableTiming)) != cudaSuccess ||
+        (ce = cudaEventCreateWithFlags(&eng->copied2, cudaEventDisableTiming)) != cudaSuccess) {
       st = fail(KITES_ERR_CUDA, "stream/event creation failed: %s", cudaGetErrorString(ce));
       break;
     }
@@ -2054,6 +2066,7 @@ extern "C" int kites_engine_destroy(kites_engine *eng) {
   cudaSetDevice(eng->device);
   if (eng->stream) cudaStreamSynchronize(eng->stream);
   if (eng->copy_stream) cudaStreamSynchronize(eng->copy_stream);
+  if (eng->copy_stream2) cudaStreamSynchronize(eng->copy_stream2);
   // Graphs die with their engine; their handles are invalid afterwards.
   while (!eng->graphs.empty()) kites_graph_destroy(eng->graphs.back());
   if (eng->pinned) cudaFreeHost(eng->pinned);
@@ -2065,7 +2078,9 @@ extern "C" int kites_engine_destroy(kites_engine *eng) {
   if (eng->kev1) cudaEventDestroy(eng->kev1);
   if (eng->staged) cudaEventDestroy(eng->staged);
   if (eng->copied) cudaEventDestroy(eng->copied);
+  if (eng->copied2) cudaEventDestroy(eng->copied2);
   if (eng->copy_stream) cudaStreamDestroy(eng->copy_stream);
+  if (eng->copy_stream2) cudaStreamDestroy(eng->copy_stream2);
   if (eng->stream) cudaStreamDestroy(eng->stream);
   if (eng->pool) cudaMemPoolDestroy(eng->pool);
   delete eng;
@@ -2102,6 +2117,7 @@ extern "C" int kites_engine_sync(kites_engine *eng) {
   KITES_TRY(set_device(eng));
   KITES_CUDA_TRY(cudaStreamSynchronize(eng->stream));
   KITES_CUDA_TRY(cudaStreamSynchronize(eng->copy_stream));
+  KITES_CUDA_TRY(cudaStreamSynchronize(eng->copy_stream2));
   return KITES_OK;
 }
 
@@ -2110,7 +2126,9 @@ extern "C" int kites_engine_join(kites_engine *eng) {
   if (!eng) return fail(KITES_ERR_INVALID, "null engine");
   KITES_TRY(set_device(eng));
   KITES_CUDA_TRY(cudaEventRecord(eng->copied, eng->copy_stream));
+  KITES_CUDA_TRY(cudaEventRecord(eng->copied2, eng->copy_stream2));
   KITES_CUDA_TRY(cudaStreamWaitEvent(eng->stream, eng->copied, 0));
+  KITES_CUDA_TRY(cudaStreamWaitEvent(eng->stream, eng->copied2, 0));
   return KITES_OK;
 }
 
@@ -2118,6 +2136,7 @@ extern "C" int kites_graph_destroy(kites_graph *g) {
   if (!g) return KITES_OK;
   cudaSetDevice(g->eng->device);
   cudaStreamSynchronize(g->eng->copy_stream);
+  cudaStreamSynchronize(g->eng->copy_stream2);
   cudaStreamSynchronize(g->eng->stream);
   for (auto &kv : g->loops) {
     cudaGraphExecDestroy(kv.second.second);

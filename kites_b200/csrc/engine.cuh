@@ -17,7 +17,8 @@ struct kites_engine {
   // Asynchronous batch results: device-to-host copies run on copy_stream
   // (staged = the staging buffer holds a result, copied = its copy is done).
   cudaStream_t copy_stream = nullptr;
-  cudaEvent_t staged = nullptr, copied = nullptr;
+  cudaStream_t copy_stream2 = nullptr;  // the second half of each copy
+  cudaEvent_t staged = nullptr, copied = nullptr, copied2 = nullptr;
   cudaMemPool_t pool = nullptr;   // stream-ordered pool owning every buffer
   int sm_count = 0;
   int l2_bytes = 0;
