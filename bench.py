@@ -95,6 +95,10 @@ def parse():
     ap.add_argument("--no-lambda", action="store_true",
                     help="skip the kites::process user-function leg (examples/sssp_binary_csc)")
     ap.add_argument("--lambda-sources", type=int, default=4)
+    ap.add_argument("--suite", action="store_true",
+                    help="instead of the headline, one JSON line per other configuration: "
+                         "config 1 through kites_process, BFS / CC / PageRank, 256 sources on "
+                         "R-MAT scale 20, the 1,000-graph batch, an Erdos-Renyi graph")
     ap.add_argument("--batch-selector", default=None,
                     help="load the batched selector's weights from this file (1628 float32) "
                          "instead of the compiled-in default")
@@ -721,10 +725,128 @@ def run_ours(args):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# the other configurations (--suite)
+# ---------------------------------------------------------------------------
+
+def run_suite(args):
+    """One line per configuration, each timed on the device (CUDA events of
+    the engine, device loop) after one untimed run; results are checked
+    against a second strategy or the plain kernel where one exists."""
+    from kites_b200 import capi
+
+    eng = capi.Engine(0)
+    lines = []
+
+    def emit(workload, value, unit, **kw):
+        rec = {"suite": True, "workload": workload, "value": value, "unit": unit, **kw}
+        lines.append(rec)
+        print(json.dumps(rec), flush=True)
+
+    def timed(fn, reps):
+        fn()
+        return min(fn() for _ in range(reps))
+
+    # Config 1: 7,115 vertices, 103,689 edges, SSSP from vertex 0 through
+    # kites_process (the reference's process() call), weights U[1,63].
+    s, d, w = capi.gen_rmat(13, 103689, seed=1, w_lo=1, w_hi=63, n_vertices=7115)
+    R, C, E = capi.csc_from_edges(7115, s, d, w)
+    g = capi.Graph(eng, R, C, E)
+    outdeg = np.bincount(C, minlength=7115).astype(np.uint64)
+    dist, _ = g.sssp(0)
+    reach = reached_edges(dist, outdeg)
+    for loop in (1, 0):
+        ms = timed(lambda: g.sssp(0, out=False, opts=capi.default_opts(device_loop=loop))[1]
+                   .device_ms, 20)
+        emit("cfg1_sssp", reach / (ms * 1e-3) / 1e9, UNIT, ms=ms,
+             loop="device (CUDA graph)" if loop else "host (flag read back per iteration)")
+    g.close()
+
+    # Scale 22, R-MAT and Erdos-Renyi: plain SSSP and BFS from 8 sources,
+    # min-label CC on the symmetrised graph.
+    n = 1 << 22
+    for kind in ("rmat22", "er22"):
+        if kind == "rmat22":
+            s, d, w = capi.gen_rmat(22, 16 * n, seed=1)
+        else:
+            s, d, w = capi.gen_er(n, 16 * n, seed=1)
+        R, C, E = capi.csc_from_edges(n, s, d, w)
+        g = capi.Graph(eng, R, C, E)
+        outdeg = np.bincount(C, minlength=n).astype(np.uint64)
+        srcs = pick_sources(outdeg, 8, args.seed)
+        for op, name in ((capi.OP_SSSP, "sssp"), (capi.OP_BFS, "bfs")):
+            for strat, sname in ((capi.STRATEGY_PLAIN, "plain"), (capi.STRATEGY_AUTO, "auto")):
+                o = capi.default_opts(strategy=strat)
+                tot_ms, tot_e = 0.0, 0
+                for src in srcs:
+                    dist, st = g.sssp(int(src), op=op, opts=o)
+                    tot_ms += timed(lambda: g.sssp(int(src), op=op, out=False, opts=o)[1]
+                                    .device_ms, 2)
+                    tot_e += reached_edges(dist, outdeg)
+                emit(f"{kind}_{name}", tot_e / (tot_ms * 1e-3) / 1e9, UNIT, sources=len(srcs),
+                     strategy=sname, ms_per_source=tot_ms / len(srcs))
+        g.close()
+        gs = capi.Graph.from_edges(eng, n, np.concatenate([s, d]), np.concatenate([d, s]),
+                                   directed=False)
+        for strat, sname in ((capi.STRATEGY_PLAIN, "plain"), (capi.STRATEGY_PUSH, "push")):
+            o = capi.default_opts(strategy=strat)
+            ms = timed(lambda: gs.cc(opts=o)[1].device_ms, 2)
+            emit(f"{kind}_cc", 2 * s.shape[0] / (ms * 1e-3) / 1e9, "GTEPS (edges of the "
+                 "symmetrised graph per run)", ms=ms, strategy=sname)
+        gs.close()
+        del s, d, w, R, C, E
+
+    # 256 seeded sources on R-MAT scale 20 as one K = 256 batch.
+    n = 1 << 20
+    s, d, w = capi.gen_rmat(20, 16 * n, seed=1)
+    R, C, E = capi.csc_from_edges(n, s, d, w)
+    g = capi.Graph(eng, R, C, E)
+    outdeg = np.bincount(C, minlength=n).astype(np.uint64)
+    srcs = pick_sources(outdeg, 256, args.seed)
+    out = np.empty((n, 256), np.uint32)
+    want = None
+    for strat, sname in ((capi.STRATEGY_PLAIN, "plain"), (capi.STRATEGY_AUTO, "auto")):
+        o = capi.default_opts(strategy=strat)
+        g.sssp_batch(srcs, out=out, opts=o)
+        if want is None:
+            want = out.copy()
+            reach = sum(reached_edges(want[:, j], outdeg) for j in range(256))
+        ok = bool(np.array_equal(out, want))
+        ms = timed(lambda: g.sssp_batch(srcs, out=out, opts=o)[1].device_ms, 2)
+        emit("rmat20_batch256", reach / (ms * 1e-3) / 1e9, UNIT, ms=ms, strategy=sname,
+             bit_exact_vs_plain=ok)
+    # PageRank, 20 iterations (GTEPS = 20 m / time).
+    ms = timed(lambda: g.pagerank(iterations=20)[1].device_ms, 2)
+    emit("rmat20_pagerank20", 20 * C.shape[0] / (ms * 1e-3) / 1e9, "GTEPS (20 m per run)",
+         ms=ms)
+    g.close()
+    del s, d, w, R, C, E, out, want
+
+    # 1,000 R-MAT graphs (vertices log-uniform in [1K, 100K], edge factor
+    # U[4, 32]) as one disjoint union, one seed (vertex 0 of each) per graph,
+    # one device loop.
+    s, d, w, vo, eo = capi.gen_rmat_union(1000, seed=1)
+    nn = int(vo[-1])
+    R, C, E = capi.csc_from_edges(nn, s, d, w)
+    g = capi.Graph(eng, R, C, E)
+    seeds = vo[:-1].astype(np.uint32)
+    dist, _ = g.sssp_multi_seed(seeds)
+    outdeg = np.bincount(C, minlength=nn).astype(np.uint64)
+    reach = reached_edges(dist, outdeg)
+    ms = timed(lambda: g.sssp_multi_seed(seeds, out=False)[1].device_ms, 3)
+    emit("multigraph1000_sssp", reach / (ms * 1e-3) / 1e9, UNIT, ms=ms, graphs=1000,
+         vertices=nn, edges=int(eo[-1]))
+    g.close()
+    eng.close()
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.suite:
+        return run_suite(args)
     return run_ours(args)
 
 

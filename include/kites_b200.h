@@ -54,8 +54,9 @@ typedef enum kites_op {
  * when the predicted gain is under the margin.  The others force one
  * strategy for every iteration (used to record training timings).
  * Batched runs (kites_sssp_batch) take PLAIN, AUTO, PUSH, PULL_ALL and
- * PULL_CHANGED; there PUSH, PULL_ALL and PULL_CHANGED move only the 32-byte
- * sectors of each source row that changed in the previous iteration. */
+ * PULL_CHANGED; there PUSH and PULL_CHANGED move only the 32-byte sectors of
+ * each source row that changed in the previous iteration, and PULL_ALL
+ * pulls every row without an activation pass. */
 typedef enum kites_strategy {
   KITES_STRATEGY_PLAIN = 0,
   KITES_STRATEGY_AUTO = 1,

@@ -1468,7 +1468,8 @@ int dispatch_batch(kites_graph *g, int op, const uint32_t *src, uint32_t k, uint
 //                 over A with whole source rows (k_pull_batch);
 //   PULL_CHANGED  the same frontier, gathering only the changed sectors of
 //                 each source (k_pull_batch<masked>);
-//   PULL_ALL      every row, changed sectors only, no activation pass;
+//   PULL_ALL      every row over whole source rows, no activation pass (the
+//                 dense iterations' frontier is nearly every row anyway);
 //   PUSH          the out-edges of U's rows relax the changed sectors of
 //                 their targets with atomicMin (k_push_batch).
 // AUTO lets the selector pick per iteration (k_select with the batched
@@ -1586,8 +1587,10 @@ int launch_batch_strategy(kites_graph *g, const batch_flex &f, int strategy, int
       break;
     }
     case KITES_STRATEGY_PULL_ALL: {
+      // Every row over whole source rows: no activation pass, and exact
+      // without the changed-sector invariant (every in-edge is folded).
       pull_batch_args<OffT> pa{gb, (const uint32_t *)g->E, f.D, nullptr, Un, g->ctr, Mc, Mn};
-      k_pull_batch<OP, OffT, K, true><<<f.mpull_grid, kBlock, 0, s>>>(pa);
+      k_pull_batch<OP, OffT, K, false><<<f.pull_grid, kBlock, 0, s>>>(pa);
       break;
     }
     case KITES_STRATEGY_PUSH: {

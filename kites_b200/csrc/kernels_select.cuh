@@ -24,7 +24,15 @@ struct select_acc {
   unsigned long long cnt, osum, isum;
   unsigned int omax, blocks_done;
   unsigned long long msum;   // batched: changed sectors of the changed rows
+  unsigned int imax, pad;    // largest in-degree of a changed row
 };
+
+// Guard of the threads-per-vertex class: it walks each row with one group
+// of at most 32 lanes, so a row of this many in-edges or more (a hub of a
+// power-law graph) holds its group far longer than an edge-balanced chunk;
+// the class is not picked while the changed set holds such a row, whatever
+// the model predicts.
+constexpr unsigned int kTpvMaxRow = 8192;
 
 template <typename OffT>
 struct select_args {
@@ -82,11 +90,11 @@ __global__ void __launch_bounds__(256) k_select(select_args<OffT> a) {
     return;
   }
   __shared__ unsigned long long s_c[8], s_o[8], s_i[8], s_s[8];
-  __shared__ unsigned int s_m[8];
+  __shared__ unsigned int s_m[8], s_x[8];
   __shared__ bool last;
   __shared__ float x[kFeat], h1[kH], h2[kH], out[kClasses];
   unsigned long long c = 0, os = 0, is = 0, ms = 0;
-  unsigned int om = 0;
+  unsigned int om = 0, im = 0;
   const uint32_t lane = lane_id(), wid = threadIdx.x >> 5;
   // A warp reads 32 changed-set words at once (one coalesced load, so an
   // empty stretch costs one load per 32 words); for each non-empty word a
@@ -119,31 +127,38 @@ __global__ void __launch_bounds__(256) k_select(select_args<OffT> a) {
       for (int q = 0; q < kRound; ++q) {
         os += od[q];
         om = max(om, od[q]);
-        is += (unsigned long long)(r1[q] - r0[q]);
+        const unsigned long long deg = (unsigned long long)(r1[q] - r0[q]);
+        is += deg;
+        im = max(im, (unsigned int)min(deg, 0xFFFFFFFFull));
       }
     }
   }
   c = __reduce_add_sync(kFull, (uint32_t)c);
   om = __reduce_max_sync(kFull, om);
+  im = __reduce_max_sync(kFull, im);
 #pragma unroll
   for (int d = 16; d; d >>= 1) {
     os += __shfl_xor_sync(kFull, os, d);
     is += __shfl_xor_sync(kFull, is, d);
     ms += __shfl_xor_sync(kFull, ms, d);
   }
-  if (lane == 0) { s_c[wid] = c; s_o[wid] = os; s_i[wid] = is; s_m[wid] = om; s_s[wid] = ms; }
+  if (lane == 0) {
+    s_c[wid] = c; s_o[wid] = os; s_i[wid] = is; s_m[wid] = om; s_s[wid] = ms; s_x[wid] = im;
+  }
   __syncthreads();
   if (threadIdx.x == 0) {
     unsigned long long tc = 0, to = 0, ti = 0, ts = 0;
-    unsigned int tm = 0;
+    unsigned int tm = 0, tx = 0;
     for (int i = 0; i < (int)(blockDim.x >> 5); ++i) {
       tc += s_c[i]; to += s_o[i]; ti += s_i[i]; ts += s_s[i]; tm = max(tm, s_m[i]);
+      tx = max(tx, s_x[i]);
     }
     if (tc) {
       atomicAdd(&a.acc->cnt, tc);
       atomicAdd(&a.acc->osum, to);
       atomicAdd(&a.acc->isum, ti);
       atomicMax(&a.acc->omax, tm);
+      atomicMax(&a.acc->imax, tx);
       if (ts) atomicAdd(&a.acc->msum, ts);
     }
     __threadfence();
@@ -176,8 +191,10 @@ __global__ void __launch_bounds__(256) k_select(select_args<OffT> a) {
     }
     x[10] = log2p1((double)a.ctr->last_edges);
     x[11] = log2p1((double)a.ctr->last_active);
+    s_x[0] = atomicMax(&a.acc->imax, 0u);
     a.acc->cnt = a.acc->osum = a.acc->isum = a.acc->msum = 0ull;
     a.acc->omax = 0u;
+    a.acc->imax = 0u;
     a.acc->blocks_done = 0u;
     const unsigned long long it = a.ctr->iterations;
     if (a.feat_out && it < a.feat_cap)
@@ -188,9 +205,12 @@ __global__ void __launch_bounds__(256) k_select(select_args<OffT> a) {
   if (a.params) {
     mlp_forward_warp(a.params, x, h1, h2, out);
     if (lane == 0) {
+      // Class 3 of the single-source selector is the threads-per-vertex
+      // pull; the batched loop's class 3 (a masked pull) needs no guard.
+      const bool tpv_ok = a.M || s_x[0] < kTpvMaxRow;
       uint32_t best = 1;
       for (uint32_t k = 2; k < kClasses; ++k)
-        if (out[k] < out[best]) best = k;
+        if ((k != 3 || tpv_ok) && out[k] < out[best]) best = k;
       cls = (out[best] < out[0] - a.margin_log) ? best : 0u;
     }
   }

@@ -12,7 +12,12 @@ For each graph, a few seeded sources with out-edges run through
 kites_selector_record: at every iteration each selector class (PLAIN, PUSH,
 PULL_ALL, the graph's TPV width) runs from the same state and is timed.
 The MLP (12 -> 32 -> 32 -> 4, FP32) is trained on the device with
-kites_selector_train (full-batch Adam on the log time ratios).
+kites_selector_train (full-batch Adam on the log time ratios), each
+iteration repeated in proportion to its PLAIN time (1 to 16 times) so that
+the fit follows the iterations a run's time is made of.  --config3 N trains
+on N graphs of the selector configuration's recipe instead (four in five
+R-MAT graphs of scales 16-22 with jittered a, b, c; one in five grids of
+side 1024-4096).
 
 Held-out evaluation: SSSP from --eval-sources seeded sources on R-MAT scale
 --eval-scale (the benchmark graph's generator and parameters, a different
@@ -356,7 +361,8 @@ def main(argv=None) -> int:
     X, T = collect(eng, a.quick, a.sources_per_graph, log, a.config3)
     T = np.maximum(T, 1e-3)
     log(f"dataset: {X.shape[0]} iterations in {time.time() - t0:.1f}s")
-    params, loss = eng.selector_train(X, T, epochs=a.epochs, lr=a.lr, seed=1)
+    Xw, Tw = time_weighted(X, T)
+    params, loss = eng.selector_train(Xw, Tw, epochs=a.epochs, lr=a.lr, seed=1)
     log(f"trained: loss {loss:.4f}")
     eng.selector_load(params)
     params.astype("<f4").tofile(a.out)

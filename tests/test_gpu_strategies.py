@@ -193,3 +193,27 @@ def test_default_selector_is_trained_and_exact(cfg1_edges):
         g.close()
     finally:
         eng.close()
+
+
+def test_tpv_guard_on_hub_graph(engine):
+    """Selector weights that always want the threads-per-vertex class: on an
+    R-MAT graph whose hubs exceed the guard's row length, the iterations
+    whose changed set holds such a row run PLAIN instead, and the result is
+    the fixed point."""
+    n = 1 << 18
+    s, d, w = capi.gen_rmat(18, 16 * n, seed=5)
+    assert np.bincount(d, minlength=n).max() >= 8192
+    R, C, E = capi.csc_from_edges(n, s, d, w)
+    g = capi.Graph(engine, R, C, E)
+    src = int(np.argmax(np.bincount(s, minlength=n)))   # the biggest hub changes first
+    plain, _ = g.sssp(src)
+    engine.selector_load(forced_selector(3))
+    try:
+        for loop in (0, 1):
+            got, st = g.sssp(src, opts=capi.default_opts(strategy=capi.STRATEGY_AUTO,
+                                                         device_loop=loop))
+            np.testing.assert_array_equal(got, plain)
+            assert st.strategy_hist[capi.STRATEGY_PLAIN] > 0, list(st.strategy_hist)
+    finally:
+        engine.selector_load(forced_selector(0))
+        g.close()
