@@ -102,6 +102,9 @@ def parse():
     ap.add_argument("--batch-selector", default=None,
                     help="load the batched selector's weights from this file (1628 float32) "
                          "instead of the compiled-in default")
+    ap.add_argument("--margin", type=float, default=None,
+                    help="AUTO: the selector's fallback margin (kites_run_opts."
+                         "selector_margin) instead of the library default")
     a = ap.parse_args()
     if a.strategy is None:
         a.strategy = "auto" if a.mode == "batch" else "plain"
@@ -434,6 +437,8 @@ def run_ours(args):
     loop = 0 if args.host_loop else 1
     bopts = capi.default_opts(device_loop=loop, strategy=STRATEGIES[args.strategy])
     sopts = capi.default_opts(device_loop=loop, strategy=STRATEGIES[args.strategy])
+    if args.margin is not None:
+        bopts.selector_margin = sopts.selector_margin = args.margin
     lib = capi.load()
 
     def batched_step():
@@ -786,15 +791,58 @@ def run_suite(args):
                 emit(f"{kind}_{name}", tot_e / (tot_ms * 1e-3) / 1e9, UNIT, sources=len(srcs),
                      strategy=sname, ms_per_source=tot_ms / len(srcs))
         g.close()
+        # Both directions of every edge as a directed graph (the per-iteration
+        # strategies take directed graphs; the labels are those of the
+        # undirected graph).
         gs = capi.Graph.from_edges(eng, n, np.concatenate([s, d]), np.concatenate([d, s]),
-                                   directed=False)
-        for strat, sname in ((capi.STRATEGY_PLAIN, "plain"), (capi.STRATEGY_PUSH, "push")):
+                                   directed=True)
+        want = None
+        for strat, sname in ((capi.STRATEGY_PLAIN, "plain"), (capi.STRATEGY_PUSH, "push"),
+                             (capi.STRATEGY_AUTO, "auto")):
             o = capi.default_opts(strategy=strat)
+            labels, _ = gs.cc(opts=o)
+            if want is None:
+                want = labels.copy()
             ms = timed(lambda: gs.cc(opts=o)[1].device_ms, 2)
             emit(f"{kind}_cc", 2 * s.shape[0] / (ms * 1e-3) / 1e9, "GTEPS (edges of the "
-                 "symmetrised graph per run)", ms=ms, strategy=sname)
+                 "symmetrised graph per run)", ms=ms, strategy=sname,
+                 bit_exact_vs_plain=bool(np.array_equal(labels, want)))
         gs.close()
         del s, d, w, R, C, E
+
+    # A 2048 x 2048 grid (road-like, weights U[1, 1000]): plain, AUTO, the
+    # mipmapped frontier (blocks of one grid row) alone and as AUTO's coarse
+    # class, 4 sources each, distances checked against plain.
+    side = 2048
+    n = side * side
+    s, d, w = capi.gen_grid(side, seed=1, w_lo=1, w_hi=1000)
+    R, C, E = capi.csc_from_edges(n, s, d, w)
+    g = capi.Graph(eng, R, C, E)
+    g.build_mipmap(side)
+    outdeg = np.bincount(C, minlength=n).astype(np.uint64)
+    srcs = pick_sources(outdeg, 4, args.seed)
+    want = {}
+    for strat, coarse, sname in ((capi.STRATEGY_PLAIN, None, "plain"),
+                                 (capi.STRATEGY_AUTO, capi.STRATEGY_PULL_ALL, "auto"),
+                                 (capi.STRATEGY_MIP, None, "mip"),
+                                 (capi.STRATEGY_AUTO, capi.STRATEGY_MIP, "auto_coarse_mip")):
+        if coarse is not None:
+            g.set_coarse(coarse)
+        o = capi.default_opts(strategy=strat)
+        tot_ms, tot_e, ok = 0.0, 0, True
+        for src in srcs:
+            dist, st = g.sssp(int(src), opts=o)
+            if sname == "plain":
+                want[int(src)] = dist.copy()
+            ok = ok and bool(np.array_equal(dist, want[int(src)]))
+            tot_ms += timed(lambda: g.sssp(int(src), out=False, opts=o)[1].device_ms, 2)
+            tot_e += reached_edges(dist, outdeg)
+        emit("grid2048_sssp", tot_e / (tot_ms * 1e-3) / 1e9, UNIT, sources=len(srcs),
+             strategy=sname, ms_per_source=tot_ms / len(srcs), bit_exact_vs_plain=ok,
+             block_vertices=side)
+    g.set_coarse(capi.STRATEGY_PULL_ALL)
+    g.close()
+    del s, d, w, R, C, E
 
     # 256 seeded sources on R-MAT scale 20 as one K = 256 batch.
     n = 1 << 20

@@ -20,7 +20,7 @@
 extern "C" {
 #endif
 
-#define KITES_B200_ABI_VERSION 2
+#define KITES_B200_ABI_VERSION 3
 
 typedef enum kites_status {
   KITES_OK = 0,
@@ -68,7 +68,10 @@ typedef enum kites_strategy {
   KITES_STRATEGY_TPV32 = 7,     /* pull, one warp per active vertex          */
   KITES_STRATEGY_PULL_CHANGED = 8,  /* pull over the frontier, reading only
                                        in-neighbours that changed last time  */
-  KITES_STRATEGY_COUNT = 9
+  KITES_STRATEGY_MIP = 9,       /* pull over the vertex blocks that the graph's
+                                   block map activates (needs
+                                   kites_graph_build_mipmap)                 */
+  KITES_STRATEGY_COUNT = 10
 } kites_strategy;
 
 typedef struct kites_engine kites_engine;
@@ -347,13 +350,37 @@ int kites_selector_save_batch(kites_engine *eng, float *params, uint32_t n_param
 /* Threads-per-vertex width of the selector's TPV class for this graph
  * (KITES_STRATEGY_TPV1/4/8/32). */
 int kites_graph_set_tpv(kites_graph *g, int strategy);
+/* What the selector's coarse class (class 2) runs on this graph:
+ * KITES_STRATEGY_PULL_ALL (default) or KITES_STRATEGY_MIP (needs the block
+ * map).  The autotuner picks it on graphs with a block map. */
+int kites_graph_set_coarse(kites_graph *g, int strategy);
+
+/* ---- mipmapped frontier ------------------------------------------------
+ * The block map of kites::graph_csr_mipmapped (kites/graph/
+ * graph_csr_mipmapped.hpp:58-75, uploaded by graph_csr_mipmapped_device,
+ * graph_csr_mipmapped_device.cuh:44-64), built on the device from the
+ * uploaded CSC: blocks of block_vertices consecutive vertices, dim =
+ * ceil(n / block_vertices) rounded up to a multiple of 32 (n the vertex
+ * count padded to a multiple of 128, as graph_raw.h:174-179 pads it), and a
+ * dim x dim row-major bit matrix with bit
+ * (s / block_vertices) * dim + d / block_vertices set for every edge s -> d
+ * (bit b of the matrix is bit b % 32 of word b / 32).  dim <= 65536.
+ * KITES_STRATEGY_MIP activates, after each iteration, every vertex of every
+ * block that a block holding a changed vertex has an edge into.  Directed
+ * graphs with vertex_per_group 1.  Rebuilding replaces the map. */
+int kites_graph_build_mipmap(kites_graph *g, uint64_t block_vertices);
+/* dim of the map, and its dim * dim / 32 words if words is non-NULL
+ * (n_words: the buffer's capacity, host or device memory). */
+int kites_graph_get_mipmap(kites_graph *g, uint64_t *dim_out, uint32_t *words,
+                           uint64_t n_words);
 
 /* ---- autotuner ---------------------------------------------------------
  * No reference counterpart (the reference fixes 128 threads per block and
  * one vertex per thread).  Times candidate tile shapes on this graph with
  * the given sources and keeps the fastest: the batched kernel's chunk size
  * (vertices + edges per warp), the threads-per-vertex width of the
- * selector's TPV class, and the frontier densities at which the plain loop
+ * selector's TPV class, its coarse class (PULL_ALL or MIP, on graphs with a
+ * block map), and the frontier densities at which the plain loop
  * switches its pull and its activation to the staged sweeps. */
 typedef struct kites_tune_result {
   uint32_t batch_chunk_items;
@@ -364,6 +391,8 @@ typedef struct kites_tune_result {
   float plain_ms;          /* best plain single-source run time */
   float tpv_ms;            /* best TPV single-source run time   */
   uint32_t trials;
+  int32_t coarse_strategy; /* the selector's coarse class: PULL_ALL or MIP */
+  float coarse_ms;         /* its AUTO run time (graphs with a block map) */
 } kites_tune_result;
 
 int kites_autotune(kites_engine *eng, kites_graph *g, int op, const uint32_t *sources,

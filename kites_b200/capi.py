@@ -21,8 +21,8 @@ LIB_PATH = os.path.join(HERE, "libkites_b200.so")
 OK, ERR_INVALID, ERR_OOM, ERR_CUDA, ERR_TIMEOUT, ERR_UNSUPPORTED, ERR_NO_DEVICE = range(7)
 OP_SSSP, OP_SSSP_WRAP, OP_BFS, OP_CC, OP_PAGERANK = range(5)
 (STRATEGY_PLAIN, STRATEGY_AUTO, STRATEGY_PUSH, STRATEGY_PULL_ALL, STRATEGY_TPV1,
- STRATEGY_TPV4, STRATEGY_TPV8, STRATEGY_TPV32, STRATEGY_PULL_CHANGED) = range(9)
-STRATEGY_COUNT = 9
+ STRATEGY_TPV4, STRATEGY_TPV8, STRATEGY_TPV32, STRATEGY_PULL_CHANGED, STRATEGY_MIP) = range(10)
+STRATEGY_COUNT = 10
 MAX_RECORDED_ITERS = 4096
 INF = 0xFFFFFFFF
 
@@ -41,7 +41,8 @@ EXPORTED = [
     "kites_graph_set_batch_gather", "kites_csc_save", "kites_csc_info", "kites_csc_load",
     "kites_selector_fit", "kites_selector_record_batch", "kites_selector_load_batch",
     "kites_selector_save_batch", "kites_graph_activate", "kites_sssp_batch_async",
-    "kites_engine_join",
+    "kites_engine_join", "kites_graph_build_mipmap", "kites_graph_get_mipmap",
+    "kites_graph_set_coarse",
 ]
 # Selector classes of the batched loop (kites_sssp_batch with AUTO).
 BATCH_CLASS_STRATEGY = [STRATEGY_PLAIN, STRATEGY_PUSH, STRATEGY_PULL_ALL, STRATEGY_PULL_CHANGED]
@@ -49,6 +50,8 @@ SELECTOR_FEATURES, SELECTOR_CLASSES, SELECTOR_PARAMS = 12, 4, 1628
 # Parameter layout of the selector MLP (offsets into the 1628 floats).
 SEL_OFF = {"mean": 0, "std": 12, "W1": 24, "b1": 408, "W2": 440, "b2": 1464, "W3": 1496,
            "b3": 1624}
+# Class 2 is the graph's coarse class (PULL_ALL unless set to MIP), class 3
+# its threads-per-vertex width.
 CLASS_STRATEGY = [STRATEGY_PLAIN, STRATEGY_PUSH, STRATEGY_PULL_ALL, None]  # None: graph's TPV
 
 
@@ -109,6 +112,7 @@ class TuneResult(Structure):
         ("batch_chunk_items", c_uint32), ("tpv_strategy", c_int32),
         ("dense_edges", c_uint64), ("dense_rows", c_uint64), ("batch_ms", c_float),
         ("plain_ms", c_float), ("tpv_ms", c_float), ("trials", c_uint32),
+        ("coarse_strategy", c_int32), ("coarse_ms", c_float),
     ]
 
 
@@ -188,6 +192,9 @@ def load(path: str = LIB_PATH):
         "kites_sssp_batch_async": (c_int, [vp, vp, c_int, vp, u32, vp, POINTER(RunOpts),
                                            POINTER(RunStats)]),
         "kites_engine_join": (c_int, [vp]),
+        "kites_graph_build_mipmap": (c_int, [vp, u64]),
+        "kites_graph_get_mipmap": (c_int, [vp, POINTER(c_uint64), vp, u64]),
+        "kites_graph_set_coarse": (c_int, [vp, c_int]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)
@@ -490,6 +497,23 @@ class Graph:
 
     def set_tpv(self, strategy):
         _check(load().kites_graph_set_tpv(self._h, strategy))
+
+    def set_coarse(self, strategy):
+        """The selector's coarse class: STRATEGY_PULL_ALL or STRATEGY_MIP."""
+        _check(load().kites_graph_set_coarse(self._h, strategy))
+
+    def build_mipmap(self, block_vertices):
+        """Block map of the mipmapped frontier (STRATEGY_MIP), built on the device."""
+        _check(load().kites_graph_build_mipmap(self._h, int(block_vertices)))
+
+    def mipmap(self):
+        """(dim, words): the block map as dim * dim / 32 uint32 words."""
+        dim = c_uint64()
+        _check(load().kites_graph_get_mipmap(self._h, ctypes.byref(dim), None, 0))
+        words = np.zeros(dim.value * dim.value // 32, dtype=np.uint32)
+        _check(load().kites_graph_get_mipmap(self._h, ctypes.byref(dim), _p(words),
+                                             words.shape[0]))
+        return dim.value, words
 
     def autotune(self, sources, batch=64, op=OP_SSSP):
         src = np.ascontiguousarray(sources, dtype=np.uint32)

@@ -16,6 +16,7 @@
 #include "kernels.cuh"
 #include "kernels_batch.cuh"
 #include "kernels_batch_tma.cuh"
+#include "kernels_mip.cuh"
 #include "kernels_pr.cuh"
 #include "kernels_select.cuh"
 #include "kernels_strategy.cuh"
@@ -796,6 +797,23 @@ int launch_strategy(kites_graph *g, const flex_state &f, int strategy, int parit
       k_pull_all<OP, OffT><<<g->pull_grid, kBlock, 0, s>>>(pa);
       break;
     }
+    case KITES_STRATEGY_MIP: {
+      // Coarse activation through the block map, then the frontier pull.
+      const mip_geom mg{g->mip, g->mip_dim, g->mip_dim / 32, g->mip_block};
+      uint32_t *bchg = g->mip_blocks, *bact = g->mip_blocks + mg.row_words;
+      const uint64_t top = std::max<uint64_t>(nw, mg.row_words);
+      k_mip_blocks<<<grid_for(top, 256, 2048), 256, 0, s>>>(Ucur, nw, mg, bchg, bact);
+      const unsigned gx = (unsigned)((mg.row_words + 255) / 256);
+      const unsigned gy = (unsigned)std::min<uint64_t>(
+          mg.row_words, std::max<uint64_t>(1, (uint64_t)g->eng->sm_count * 8 / gx));
+      k_mip_activate<<<dim3(gx, gy), 256, 0, s>>>(mg, bchg, bact);
+      k_mip_expand<<<grid_for(top, 256, 2048), 256, 0, s>>>(f.A, nw, mg, bact, bchg);
+      pull_args<OffT> pa{gin, (const uint32_t *)g->E, (uint32_t *)g->V, f.A, Unext, 0, g->ctr,
+                         nullptr, 0u, 0u, 0ull, 0ull};
+      k_pull_chunked<OP, OffT><<<g->pull_grid, kBlock, 0, s>>>(pa);
+      *launches += 3;
+      break;
+    }
     case KITES_STRATEGY_TPV1:
     case KITES_STRATEGY_TPV4:
     case KITES_STRATEGY_TPV8:
@@ -891,7 +909,7 @@ int dispatch_flex(kites_graph *g, int op, const kites_run_opts &o, kites_run_sta
 int class_strategy(const kites_graph *g, uint32_t cls) {
   switch (cls) {
     case 1: return KITES_STRATEGY_PUSH;
-    case 2: return KITES_STRATEGY_PULL_ALL;
+    case 2: return g->coarse_strategy;
     case 3: return g->tpv_strategy;
     default: return KITES_STRATEGY_PLAIN;
   }
@@ -2480,6 +2498,9 @@ static int run_strategies(kites_engine *eng, kites_graph *g, int op, const kites
     return fail(KITES_ERR_UNSUPPORTED, "SSSP needs 4-byte edge values");
   if (o.strategy < KITES_STRATEGY_PLAIN || o.strategy >= KITES_STRATEGY_COUNT)
     return fail(KITES_ERR_INVALID, "unknown strategy %d", o.strategy);
+  if (o.strategy == KITES_STRATEGY_MIP && !g->mip)
+    return fail(KITES_ERR_INVALID,
+                "KITES_STRATEGY_MIP needs the graph's block map (kites_graph_build_mipmap)");
   if (o.strategy == KITES_STRATEGY_AUTO)
     return g->off64 ? dispatch_auto<uint64_t>(g, op, o, stats)
                     : dispatch_auto<uint32_t>(g, op, o, stats);
@@ -2941,7 +2962,21 @@ extern "C" int kites_autotune(kites_engine *eng, kites_graph *g, int op, const u
     out->tpv_ms = best;
   }
   out->tpv_strategy = g->tpv_strategy;
-  // 3. Chunk size of the batched kernel.
+  // 3. The selector's coarse class: PULL_ALL or, on a graph with a block
+  // map, the mipmapped frontier, timed as whole AUTO runs; MIP must win by
+  // 2 % to replace PULL_ALL.
+  if (g->mip && g->vpg == 1 && g->directed) {
+    float t_all = 0.f, t_mip = 0.f;
+    KITES_TRY(kites_graph_set_coarse(g, KITES_STRATEGY_PULL_ALL));
+    KITES_TRY(time_single(KITES_STRATEGY_AUTO, &t_all));
+    KITES_TRY(kites_graph_set_coarse(g, KITES_STRATEGY_MIP));
+    KITES_TRY(time_single(KITES_STRATEGY_AUTO, &t_mip));
+    const bool mip = t_mip < 0.98f * t_all;
+    KITES_TRY(kites_graph_set_coarse(g, mip ? KITES_STRATEGY_MIP : KITES_STRATEGY_PULL_ALL));
+    out->coarse_ms = mip ? t_mip : t_all;
+  }
+  out->coarse_strategy = g->coarse_strategy;
+  // 4. Chunk size of the batched kernel.
   if (batch == 16 || batch == 32 || batch == 64 || batch == 128 || batch == 256) {
     std::vector<uint32_t> bs(batch);
     for (uint32_t i = 0; i < batch; ++i) bs[i] = src[i % n_sources];
@@ -2975,6 +3010,89 @@ extern "C" int kites_graph_set_batch_gather(kites_graph *g, int mode) {
   KITES_CUDA_TRY(cudaStreamSynchronize(g->eng->stream));
   g->batch_gather = mode;
   drop_batch_loops(g);  // captured loops hold the kernel choice
+  return KITES_OK;
+}
+
+// ---- block map (mipmapped frontier) ------------------------------------------
+
+extern "C" int kites_graph_build_mipmap(kites_graph *g, uint64_t block_vertices) {
+  clear_error();
+  if (!g) return fail(KITES_ERR_INVALID, "null graph");
+  if (g->vpg != 1 || !g->directed)
+    return fail(KITES_ERR_UNSUPPORTED,
+                "the block map needs a directed graph with vertex_per_group 1");
+  if (block_vertices == 0) return fail(KITES_ERR_INVALID, "block_vertices must be >= 1");
+  if (g->n_given == 0) return fail(KITES_ERR_INVALID, "empty graph");
+  // graph_csr_mipmapped.hpp:58-60: ceil(n / block), then up to a multiple of
+  // 32, n the vertex count padded to a multiple of 128 as graph_raw pads it
+  // (graph_raw.h:174-179) and as the engine holds it.
+  uint64_t dim = (g->n + block_vertices - 1) / block_vertices;
+  dim = (dim + 31) / 32 * 32;
+  if (dim > kMaxMipDim)
+    return fail(KITES_ERR_INVALID,
+                "block map of %llu x %llu bits is over the %llu x %llu limit; take larger blocks",
+                (unsigned long long)dim, (unsigned long long)dim,
+                (unsigned long long)kMaxMipDim, (unsigned long long)kMaxMipDim);
+  KITES_TRY(set_device(g->eng));
+  cudaStream_t s = g->eng->stream;
+  KITES_CUDA_TRY(cudaStreamSynchronize(s));
+  drop_all_loops(g);   // captured loops hold the old map
+  graph_release(g, g->mip);
+  graph_release(g, g->mip_blocks);
+  g->mip = g->mip_blocks = nullptr;
+  g->mip_dim = g->mip_block = 0;
+  if (g->coarse_strategy == KITES_STRATEGY_MIP) g->coarse_strategy = KITES_STRATEGY_PULL_ALL;
+  const uint64_t words = dim * dim / 32;
+  void *p = nullptr, *q = nullptr;
+  KITES_TRY(graph_alloc(g, &p, words * 4));
+  KITES_TRY(graph_alloc(g, &q, dim / 32 * 2 * 4));
+  KITES_CUDA_TRY(cudaMemsetAsync(p, 0, words * 4, s));
+  KITES_CUDA_TRY(cudaMemsetAsync(q, 0, dim / 32 * 2 * 4, s));
+  const mip_geom mg{(uint32_t *)p, dim, dim / 32, block_vertices};
+  const unsigned grid = grid_for(g->n * 32, 256, g->eng->sm_count * 16);
+  if (g->off64)
+    k_mip_build<uint64_t><<<grid, 256, 0, s>>>((const uint64_t *)g->R, g->C, g->n, mg);
+  else
+    k_mip_build<uint32_t><<<grid, 256, 0, s>>>((const uint32_t *)g->R, g->C, g->n, mg);
+  KITES_CUDA_TRY(cudaGetLastError());
+  KITES_CUDA_TRY(cudaStreamSynchronize(s));
+  g->mip = (uint32_t *)p;
+  g->mip_blocks = (uint32_t *)q;
+  g->mip_dim = dim;
+  g->mip_block = block_vertices;
+  return KITES_OK;
+}
+
+extern "C" int kites_graph_get_mipmap(kites_graph *g, uint64_t *dim_out, uint32_t *words,
+                                      uint64_t n_words) {
+  clear_error();
+  if (!g) return fail(KITES_ERR_INVALID, "null graph");
+  if (!g->mip) return fail(KITES_ERR_INVALID, "the graph has no block map");
+  if (dim_out) *dim_out = g->mip_dim;
+  if (!words) return KITES_OK;
+  const uint64_t total = g->mip_dim * g->mip_dim / 32;
+  if (n_words < total)
+    return fail(KITES_ERR_INVALID, "the block map has %llu words, the buffer %llu",
+                (unsigned long long)total, (unsigned long long)n_words);
+  KITES_TRY(set_device(g->eng));
+  KITES_CUDA_TRY(cudaMemcpyAsync(words, g->mip, total * 4, cudaMemcpyDefault, g->eng->stream));
+  KITES_CUDA_TRY(cudaStreamSynchronize(g->eng->stream));
+  return KITES_OK;
+}
+
+extern "C" int kites_graph_set_coarse(kites_graph *g, int strategy) {
+  clear_error();
+  if (!g) return fail(KITES_ERR_INVALID, "null graph");
+  if (strategy != KITES_STRATEGY_PULL_ALL && strategy != KITES_STRATEGY_MIP)
+    return fail(KITES_ERR_INVALID, "the coarse class is PULL_ALL or MIP, not %d", strategy);
+  if (strategy == KITES_STRATEGY_MIP && !g->mip)
+    return fail(KITES_ERR_INVALID, "MIP needs the graph's block map (kites_graph_build_mipmap)");
+  if (g->coarse_strategy != strategy) {
+    KITES_TRY(set_device(g->eng));
+    KITES_CUDA_TRY(cudaStreamSynchronize(g->eng->stream));
+    drop_all_loops(g);   // cached AUTO loops captured the old class
+    g->coarse_strategy = strategy;
+  }
   return KITES_OK;
 }
 

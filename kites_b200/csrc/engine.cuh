@@ -117,6 +117,13 @@ struct kites_graph {
   void *sacc = nullptr;              // selector frontier-count accumulators
   uint8_t *rec_sel = nullptr;        // selector class per iteration (device)
   int tpv_strategy = KITES_STRATEGY_TPV8;   // the selector's threads-per-vertex class
+  int coarse_strategy = KITES_STRATEGY_PULL_ALL;  // the selector's coarse class (or MIP)
+  // Block map of the mipmapped frontier (KITES_STRATEGY_MIP): mip_dim x
+  // mip_dim bits, row = source block; mip_blocks holds the changed-block and
+  // active-block bitmaps (mip_dim / 32 words each).
+  uint32_t *mip = nullptr;
+  uint32_t *mip_blocks = nullptr;
+  uint64_t mip_dim = 0, mip_block = 0;
   float auto_margin = -1.f;          // margin the cached AUTO loop was captured with
   float auto_margin_batch = -1.f;    // the same for the batched AUTO loops
 

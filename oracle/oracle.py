@@ -258,18 +258,26 @@ def mipmap_of(hg: HostGraph, cr: int):
     s -> d.  Returns (mipmapDim, frontier words, mipmap words)."""
     assert hg.directed and hg.vertexPerGroup == 1 and cr > 0
     n = hg.n_vertices
-    dim = -(-n // cr)
-    dim = -(-dim // 32) * 32
     act = np.flatnonzero(unpack_bits(hg.vBitmap, hg.nbits)[:n])
-    blocks = np.zeros(dim, dtype=bool)
-    blocks[act // cr] = True
     counts = np.diff(hg.dir_R.astype(np.int64))
     src = np.repeat(np.arange(n, dtype=np.int64), counts)
-    bit = (src // cr) * dim + hg.dir_C.astype(np.int64) // cr
+    dim, words = mipmap_from_edges(n, src, hg.dir_C, cr)
+    blocks = np.zeros(dim, dtype=bool)
+    blocks[act // cr] = True
+    return dim, _pack_bits(blocks), words
+
+
+def mipmap_from_edges(n: int, src, dst, cr: int):
+    """The mipmap of mipmap_of for an edge list s -> d over n vertices:
+    (mipmapDim, dim * dim / 32 words), bit (s // cr) * dim + d // cr
+    (graph_csr_mipmapped.hpp:58-75)."""
+    dim = -(-n // cr)
+    dim = -(-dim // 32) * 32
+    bit = (np.asarray(src, dtype=np.int64) // cr) * dim + np.asarray(dst, dtype=np.int64) // cr
     words = np.zeros(dim * dim // 32, dtype=np.uint32)
     bit = np.unique(bit)
     np.bitwise_or.at(words, bit >> 5, (np.uint32(1) << (bit & 31).astype(np.uint32)))
-    return dim, _pack_bits(blocks), words
+    return dim, words
 
 
 def example_weight_rule(src, dst):

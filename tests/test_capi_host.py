@@ -38,7 +38,7 @@ def test_exports_every_declared_symbol():
 
 
 def test_abi_version():
-    assert capi.load().kites_abi_version() == 2
+    assert capi.load().kites_abi_version() == 3
 
 
 def test_struct_layout_matches_header():
@@ -54,6 +54,9 @@ int main(void) {
   P(kites_device_view, stream) P(kites_device_view, chunk_items) P(kites_run_opts, time_kernels)
   P(kites_run_stats, pull_kernel_bytes) P(kites_run_stats, iter_edges)
   P(kites_run_stats, pull_dense_bytes) P(kites_csc_view, offsets64)
+  printf("tune %zu\n", sizeof(kites_tune_result));
+  P(kites_tune_result, coarse_strategy) P(kites_tune_result, coarse_ms)
+  printf("strategies %d\n", (int)KITES_STRATEGY_COUNT);
   return 0;
 }
 """
@@ -77,6 +80,10 @@ int main(void) {
     assert int(got["kites_run_stats.iter_edges"]) == capi.RunStats.iter_edges.offset
     assert int(got["kites_run_stats.pull_dense_bytes"]) == capi.RunStats.pull_dense_bytes.offset
     assert int(got["kites_csc_view.offsets64"]) == capi.CscView.offsets64.offset
+    assert int(got["tune"]) == ctypes.sizeof(capi.TuneResult)
+    assert int(got["kites_tune_result.coarse_strategy"]) == capi.TuneResult.coarse_strategy.offset
+    assert int(got["kites_tune_result.coarse_ms"]) == capi.TuneResult.coarse_ms.offset
+    assert int(got["strategies"]) == capi.STRATEGY_COUNT
 
 
 def test_default_opts():

@@ -114,7 +114,10 @@ def test_batched_record_fit_and_run(engine, uploaded):
         srcs = sources_for(n, 64, seed)
         x, t = g.selector_record_batch(srcs, capacity=128)
         _, st = g.sssp_batch(srcs)
-        assert x.shape[0] == st.iterations and np.all(t > 0)
+        # The pulls update D in place, so a value lowered early in an
+        # iteration can be read later in the same one: the iteration count
+        # of two runs may differ by scheduling (the distances never do).
+        assert abs(x.shape[0] - st.iterations) <= 2 and np.all(t > 0)
         X.append(x)
         T.append(t)
     single = engine.selector_save()

@@ -69,6 +69,18 @@ def test_mipmap_matches_reference_cfg1(golden, cfg1_edges, cr):
     assert h == bytes(golden[f"cfg1_mipmap_cr{cr}"])
 
 
+@pytest.mark.parametrize("cr", [1, 3, 32, 100, 1000])
+def test_mipmap_from_edges_matches_class(cfg1_edges, cr):
+    """The edge-list form the engine's block map is checked against equals the
+    class form over the padded vertex count."""
+    s, d, w = cfg1_edges
+    hg = O.build_host_graph(s, d, w, init="source", source=0, inf=EX_INF)
+    dim, _, mip = O.mipmap_of(hg, cr)
+    dim2, mip2 = O.mipmap_from_edges(hg.n_vertices, s, d, cr)
+    assert hg.n_vertices == 7168 and dim == dim2
+    np.testing.assert_array_equal(mip, mip2)
+
+
 @pytest.mark.parametrize("cr", [1, 3, 32, 100])
 def test_mipmap_matches_reference_wiki(golden, has_reference, cr):
     if not has_reference:
