@@ -90,6 +90,7 @@ def test_default_opts():
     o = capi.default_opts()
     assert o.strategy == capi.STRATEGY_PLAIN and o.device_loop == 1
     assert o.pagerank_iterations == 20 and abs(o.damping - 0.85) < 1e-7
+    assert o.selector_margin < 0   # each loop's own default margin
 
 
 def test_no_device_is_an_error_not_a_fallback():
