@@ -619,12 +619,15 @@ def run_ours(args):
         # Each batch's V x K result leaves through kites_sssp_batch_async: its
         # copy to pinned host memory runs under the next batch's compute;
         # the join puts the last copy inside the timed region.
+        returns = []
+        t_host = time.perf_counter()
         e0.record(stream)
         for _ in range(args.steps):
             for grp in groups:
                 capi._check(lib.kites_sssp_batch_async(eng._h, g._h, capi.OP_SSSP, capi._p(grp),
                                                        K, capi._p(pinned), ctypes.byref(bopts),
                                                        None))
+                returns.append(round((time.perf_counter() - t_host) * 1e3, 2))
         capi._check(lib.kites_engine_join(eng._h))
         e1.record(stream)
         torch.cuda.synchronize()
@@ -644,7 +647,7 @@ def run_ours(args):
         e2e = {"value": total_units / (e_ms * 1e-3) / 1e9, "unit": UNIT,
                "h2d_bytes_per_step": 4 * len(srcs),
                "d2h_bytes_per_step": 4 * n * len(srcs),
-               "d2h_gbs_alone": d2h_gbs}
+               "d2h_gbs_alone": d2h_gbs, "call_returns_ms": returns}
 
     # Correctness of what was timed, after the timed region: the distances of
     # the first batch (or the first sources of --mode single), column for

@@ -145,7 +145,9 @@ typedef struct kites_run_opts {
   uint64_t max_iterations;          /* 0 = until convergence                */
   uint32_t pagerank_iterations;     /* PAGERANK only (default 20)           */
   float damping;                    /* PAGERANK only (default 0.85)         */
-  float selector_margin;            /* AUTO: min predicted gain (fraction)  */
+  float selector_margin;            /* AUTO: min predicted gain (fraction);
+                                       negative (default): 0.1 single-source,
+                                       0.03 batched                          */
   int32_t record_iterations;        /* fill kites_run_stats.iter_* arrays   */
   int32_t time_kernels;             /* host loop with CUDA events around each
                                        pull launch (fills pull_kernel_*)    */

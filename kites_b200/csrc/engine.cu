@@ -807,7 +807,7 @@ int launch_strategy(kites_graph *g, const flex_state &f, int strategy, int parit
       const unsigned gy = (unsigned)std::min<uint64_t>(
           mg.row_words, std::max<uint64_t>(1, (uint64_t)g->eng->sm_count * 8 / gx));
       k_mip_activate<<<dim3(gx, gy), 256, 0, s>>>(mg, bchg, bact);
-      k_mip_expand<<<grid_for(top, 256, 2048), 256, 0, s>>>(f.A, nw, mg, bact, bchg);
+      k_mip_expand<<<grid_for(top, 256, 2048), 256, 0, s>>>(f.A, nw, g->n, mg, bact, bchg);
       pull_args<OffT> pa{gin, (const uint32_t *)g->E, (uint32_t *)g->V, f.A, Unext, 0, g->ctr,
                          nullptr, 0u, 0u, 0ull, 0ull};
       k_pull_chunked<OP, OffT><<<g->pull_grid, kBlock, 0, s>>>(pa);
@@ -1956,10 +1956,19 @@ int check_graph(kites_engine *eng, kites_graph *g) {
   return set_device(eng);
 }
 
-kites_run_opts resolve_opts(const kites_run_opts *opts) {
+// AUTO's fallback margins when the caller leaves selector_margin negative:
+// the single-source selector's classes differ by large factors and a wrong
+// pick is costly; the batched selector's differ by a few per cent in the
+// dense iterations (the pull over every row against PLAIN), and at R-MAT
+// scale 24 margins 0 to 0.05 ran 256.5-256.7 GTEPS against 242.4 at 0.1.
+constexpr float kSelectorMargin = 0.1f;
+constexpr float kSelectorMarginBatch = 0.03f;
+
+kites_run_opts resolve_opts(const kites_run_opts *opts, bool batched = false) {
   kites_run_opts o;
   kites_default_run_opts(&o);
   if (opts) o = *opts;
+  if (o.selector_margin < 0.f) o.selector_margin = batched ? kSelectorMarginBatch : kSelectorMargin;
   if (o.pagerank_iterations == 0) o.pagerank_iterations = 20;
   if (o.damping <= 0.f) o.damping = 0.85f;
   return o;
@@ -1983,7 +1992,7 @@ extern "C" void kites_default_run_opts(kites_run_opts *o) {
   o->device_loop = 1;
   o->pagerank_iterations = 20;
   o->damping = 0.85f;
-  o->selector_margin = 0.1f;
+  o->selector_margin = -1.f;   // negative: the loop's own default (resolve_opts)
 }
 
 extern "C" int kites_engine_create(int device, kites_engine **out) {
@@ -2636,7 +2645,7 @@ static int sssp_batch(kites_engine *eng, kites_graph *g, int op, const uint32_t 
   for (uint32_t i = 0; i < k; ++i)
     if (host_src[i] >= g->n_given)
       return fail(KITES_ERR_INVALID, "source %u (slot %u) out of range", host_src[i], i);
-  kites_run_opts o = resolve_opts(opts);
+  kites_run_opts o = resolve_opts(opts, true);
   if (stats) memset(stats, 0, sizeof(*stats));
   if (o.strategy != KITES_STRATEGY_PLAIN) {
     if (o.strategy != KITES_STRATEGY_AUTO && o.strategy != KITES_STRATEGY_PUSH &&

@@ -106,15 +106,17 @@ __global__ void __launch_bounds__(256) k_mip_activate(mip_geom mg, const uint32_
   if (acc) atomicOr(bact + x, acc);
 }
 
-// Active blocks -> read frontier A (vertex bits; A is clear on entry).  Also
-// clears bchg for the next MIP iteration.
-__global__ void __launch_bounds__(256) k_mip_expand(uint32_t *A, uint64_t nwords, mip_geom mg,
-                                                    const uint32_t *bact, uint32_t *bchg) {
+// Active blocks -> read frontier A (vertex bits of the n vertices; A is
+// clear on entry and has nwords >= n / 32 words).  Also clears bchg for the
+// next MIP iteration.
+__global__ void __launch_bounds__(256) k_mip_expand(uint32_t *A, uint64_t nwords, uint64_t n,
+                                                    mip_geom mg, const uint32_t *bact,
+                                                    uint32_t *bchg) {
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   const uint64_t top = max(nwords, mg.row_words);
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < top; i += stride) {
     if (i < mg.row_words) bchg[i] = 0u;
-    if (i >= nwords) continue;
+    if (i >= nwords || i * 32 >= n) continue;   // n is a multiple of 32
     const uint64_t v0 = i * 32;
     uint32_t bits = 0u;
     for (uint64_t blk = v0 / mg.block; blk * mg.block < v0 + 32 && blk < mg.dim; ++blk) {

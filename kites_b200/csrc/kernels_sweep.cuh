@@ -342,7 +342,11 @@ __global__ void __launch_bounds__(kSweepThreads, kSweepMinBlocks)
       // together with the U words (one round trip instead of two dependent
       // ones) was measured slower: 882.7 against 725.8 ms per 64 sources at
       // R-MAT scale 24, the dense sweeps at 0.36 against 0.48 of the copy
-      // peak -- the extra gathers cost more than the saved latency.
+      // peak -- the extra gathers cost more than the saved latency.  So was
+      // one gather per edge from an array holding V on U and kInf elsewhere,
+      // written before the sweep: 832.2 against 728.7 ms, with 7 % more
+      // iterations (that copy of V misses the values lowered earlier in the
+      // same iteration, which the live V read passes on at once).
       uint32_t hit[kEdgesPerThread], cand[kEdgesPerThread];
 #pragma unroll
       for (int k = 0; k < kEdgesPerThread; ++k) {

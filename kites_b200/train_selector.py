@@ -263,6 +263,35 @@ def evaluate_batch(eng, scale: int, k: int, batches: int, seed: int, log):
     return res
 
 
+def validate_batch(eng, scale: int, k: int, batches: int, seed: int, candidates, log):
+    """AUTO device time of each candidate parameter set on a validation graph
+    (the benchmark's generator with its own seed, distinct from the
+    evaluation graph's); returns the index of the fastest."""
+    n = 1 << scale
+    s, d, w = capi.gen_rmat(scale, 16 * n, 0.57, 0.19, 0.19, seed, 1, 255)
+    R, C, E = capi.csc_from_edges(n, s, d, w)
+    del s, d, w
+    outdeg = np.bincount(C, minlength=n)
+    cand = np.flatnonzero(outdeg > 0)
+    g = capi.Graph(eng, R, C, E)
+    del C, E
+    groups = [np.array([cand[splitmix(seed, 1000 * b + j) % cand.shape[0]] for j in range(k)],
+                       dtype=np.uint32) for b in range(batches)]
+    out = np.empty((n, k), np.uint32)
+    o = capi.default_opts(strategy=capi.STRATEGY_AUTO)
+    times = []
+    for i, params in enumerate(candidates):
+        eng.selector_load_batch(params)
+        g.sssp_batch(groups[0], out=out, opts=o)  # warm-up
+        total = 0.0
+        for grp in groups:
+            total += g.sssp_batch(grp, out=out, opts=o)[1].device_ms
+        times.append(total)
+        log(f"validation fit {i}: AUTO {total:.2f} ms over {batches} batches")
+    g.close()
+    return int(np.argmin(times)), times
+
+
 def evaluate(eng, scale: int, n_src: int, seed: int, log):
     n = 1 << scale
     s, d, w = capi.gen_rmat(scale, 16 * n, 0.57, 0.19, 0.19, seed, 1, 255)
@@ -326,6 +355,10 @@ def main(argv=None) -> int:
                     help="train on this many graphs of the configuration's recipe "
                          "(R-MAT 16-22 with jittered a,b,c and grids of side 1024-4096)")
     ap.add_argument("--eval-batches", type=int, default=2)
+    ap.add_argument("--fits", type=int, default=1,
+                    help="batched: fit this many seeds and keep the one whose AUTO is "
+                         "fastest on a validation graph (seed --eval-seed + 1)")
+    ap.add_argument("--valid-scale", type=int, default=23)
     a = ap.parse_args(argv)
 
     def log(msg):
@@ -338,12 +371,19 @@ def main(argv=None) -> int:
         T = np.maximum(T, 1e-3)
         log(f"dataset: {X.shape[0]} batched iterations in {time.time() - t0:.1f}s")
         Xw, Tw = time_weighted(X, T)
-        params, loss = eng.selector_fit(Xw, Tw, epochs=a.epochs, lr=a.lr, seed=1)
-        log(f"trained: loss {loss:.4f}")
+        fits = [eng.selector_fit(Xw, Tw, epochs=a.epochs, lr=a.lr, seed=1 + i)
+                for i in range(max(1, a.fits))]
+        best, val_ms = 0, None
+        if len(fits) > 1:
+            best, val_ms = validate_batch(eng, a.valid_scale, a.batch, a.eval_batches,
+                                          a.eval_seed + 1, [p for p, _ in fits], log)
+        params, loss = fits[best]
+        log(f"trained: loss {loss:.4f} (fit {best} of {len(fits)})")
         eng.selector_load_batch(params)
         params.astype("<f4").tofile(a.out)
         report = {"dataset_iterations": int(X.shape[0]), "weighted_rows": int(Xw.shape[0]),
-                  "train_loss": loss, "batch": a.batch,
+                  "train_loss": loss, "batch": a.batch, "fits": len(fits), "chosen_fit": best,
+                  "validation_auto_ms": val_ms,
                   "class_sum_ms_train": T.sum(0).tolist(),
                   "oracle_best_over_plain_train": float(T[:, 0].sum() / T.min(1).sum())}
         if a.eval_scale:

@@ -8,10 +8,8 @@ in the iteration's changed set or already satisfies V[v] <= comp(V[u]) (when u
 last changed, v was activated and pulled it).  This test runs a synchronous
 (Jacobi) model of the plain loop -- every active row folds every in-edge --
 next to the same loop whose pull folds only the in-edges from the previous
-changed set with the sources' values at the start of the iteration (what the
-kernel gathers from k_changed_values' array), on the config-1 graph and on
-random graphs, and requires the same values, active rows and traversed edges
-in every iteration."""
+changed set, on the config-1 graph and on random graphs, and requires the same
+values, active rows and traversed edges in every iteration."""
 import numpy as np
 import pytest
 
