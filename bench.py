@@ -612,13 +612,20 @@ def run_ours(args):
                "d2h_bytes_per_step": 4 * n * len(srcs)}
     elif not args.no_e2e:
         pinned = torch.empty((n, K), dtype=torch.int32, pin_memory=True)
+        # Each batch's V x K result leaves through kites_sssp_batch_async: its
+        # copy to pinned host memory runs under the next batch's compute;
+        # the join puts the last copy inside the timed region.  Untimed
+        # warm-up calls first (the first one allocates the graph's staging
+        # buffer for the asynchronous copies).
+        for _ in range(max(1, args.warmup)):
+            capi._check(lib.kites_sssp_batch_async(eng._h, g._h, capi.OP_SSSP,
+                                                   capi._p(groups[0]), K, capi._p(pinned),
+                                                   ctypes.byref(bopts), None))
+        capi._check(lib.kites_engine_sync(eng._h))
         barrier(world)
         torch.cuda.synchronize()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
-        # Each batch's V x K result leaves through kites_sssp_batch_async: its
-        # copy to pinned host memory runs under the next batch's compute;
-        # the join puts the last copy inside the timed region.
         returns = []
         t_host = time.perf_counter()
         e0.record(stream)
