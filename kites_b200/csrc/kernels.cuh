@@ -172,6 +172,20 @@ __device__ __forceinline__ bool frontier_dense(const run_counters *c, uint32_t c
 // policy; a row entirely inside the chunk stores its new value, a row split
 // over chunks merges through atomicMin; updated rows set their bit (vertex
 // or group) in chg.
+// Whether any bitmap word in [w0, w1] is non-zero: four independent loads
+// per round trip (a loop that stops at the first live word would wait for
+// each load before issuing the next).
+__device__ __forceinline__ bool any_word(const uint32_t *bits, uint64_t w0, uint64_t w1) {
+  for (uint64_t w = w0; w <= w1; w += 4) {
+    uint32_t x = bits[w];
+    if (w + 1 <= w1) x |= bits[w + 1];
+    if (w + 2 <= w1) x |= bits[w + 2];
+    if (w + 3 <= w1) x |= bits[w + 3];
+    if (x) return true;
+  }
+  return false;
+}
+
 template <int OP, typename OffT, bool kFiltered>
 __device__ __forceinline__ void pull_chunks(const pull_args<OffT> &a) {
   __shared__ uint32_t s_ex[kWarpsPerBlock][32];
@@ -199,8 +213,7 @@ __device__ __forceinline__ void pull_chunks(const pull_args<OffT> &a) {
           const uint64_t v0 = a.g.chunk_v0[c];
           uint64_t v1 = a.g.chunk_v0[c + 1];
           if (v1 >= a.g.n_rows) v1 = a.g.n_rows - 1;
-          for (uint64_t w = (v0 >> a.shift) >> 5; w <= (v1 >> a.shift) >> 5; ++w)
-            if (a.rd[w]) { live_chunk = true; break; }
+          live_chunk = any_word(a.rd, (v0 >> a.shift) >> 5, (v1 >> a.shift) >> 5);
         }
       }
     }
@@ -322,60 +335,79 @@ __global__ void __launch_bounds__(kBlock) k_expand_chunked(expand_args<OffT> a) 
   OffT *lo_s = s_lo[wib];
   uint32_t n_rows = 0, n_edges = 0;
   const uint64_t stride = (uint64_t)gridDim.x * kWarpsPerBlock;
-  for (uint64_t ch = (uint64_t)blockIdx.x * kWarpsPerBlock + wib;
-       ch < a.g.nchunks; ch += stride) {
-    const int64_t item_lo = (int64_t)(ch * a.g.chunk_items);
-    const int64_t item_hi =
-        min(item_lo + (int64_t)a.g.chunk_items, (int64_t)a.g.n_items);
-    const uint64_t r_first = a.g.chunk_v0[ch];
-    uint64_t r_last = a.g.chunk_v0[ch + 1];
-    if (r_last >= a.g.n_rows) r_last = a.g.n_rows - 1;
-    for (uint64_t rb = r_first & ~31ull; rb <= r_last; rb += 32) {
-      const uint32_t word = a.chg[rb >> 5];
-      if (word == 0) continue;
-      const uint64_t r = rb + lane;
-      const bool active =
-          r >= r_first && r <= r_last && ((word >> lane) & 1u);
-      uint32_t cnt = 0;
-      OffT elo = 0;
-      if (active) {
-        const int64_t r0 = (int64_t)a.g.R[r], r1 = (int64_t)a.g.R[r + 1];
-        const int64_t lo = max(r0, item_lo - (int64_t)r - 1);
-        const int64_t hi = min(r1, item_hi - (int64_t)r - 1);
-        cnt = hi > lo ? (uint32_t)(hi - lo) : 0u;
-        elo = (OffT)lo;
-        const int64_t rpos = (int64_t)r + r0;
-        n_rows += (rpos >= item_lo && rpos < item_hi) ? 1u : 0u;
-        n_edges += cnt;
+  // Warp gw owns chunks gw, gw + W, gw + 2W, ...; per round each lane tests
+  // one of the next 32 for a changed row and only those chunks are walked
+  // (a sparse changed set costs one round trip per 32 chunks, not one per
+  // bitmap word of every chunk).
+  const uint64_t gw = (uint64_t)blockIdx.x * kWarpsPerBlock + wib;
+  for (uint64_t cbase = gw; cbase < a.g.nchunks; cbase += stride * 32) {
+    bool live_chunk = false;
+    {
+      const uint64_t c = cbase + (uint64_t)lane * stride;
+      if (c < a.g.nchunks) {
+        const uint64_t v0 = a.g.chunk_v0[c];
+        uint64_t v1 = a.g.chunk_v0[c + 1];
+        if (v1 >= a.g.n_rows) v1 = a.g.n_rows - 1;
+        live_chunk = any_word(a.chg, v0 >> 5, v1 >> 5);
       }
-      const uint32_t incl = warp_inclusive_scan(cnt);
-      const uint32_t total = __shfl_sync(kFull, incl, 31);
-      if (total == 0) continue;
-      ex[lane] = incl - cnt;
-      lo_s[lane] = elo;
-      __syncwarp();
-      for (uint32_t base = 0; base < total; base += 32 * kUnroll) {
-        uint32_t t[kUnroll];
+    }
+    uint32_t live_mask = __ballot_sync(kFull, live_chunk);
+    while (live_mask) {
+      const uint64_t ch = cbase + (uint64_t)(__ffs(live_mask) - 1) * stride;
+      live_mask &= live_mask - 1;
+      const int64_t item_lo = (int64_t)(ch * a.g.chunk_items);
+      const int64_t item_hi =
+          min(item_lo + (int64_t)a.g.chunk_items, (int64_t)a.g.n_items);
+      const uint64_t r_first = a.g.chunk_v0[ch];
+      uint64_t r_last = a.g.chunk_v0[ch + 1];
+      if (r_last >= a.g.n_rows) r_last = a.g.n_rows - 1;
+      for (uint64_t rb = r_first & ~31ull; rb <= r_last; rb += 32) {
+        const uint32_t word = a.chg[rb >> 5];
+        if (word == 0) continue;
+        const uint64_t r = rb + lane;
+        const bool active =
+            r >= r_first && r <= r_last && ((word >> lane) & 1u);
+        uint32_t cnt = 0;
+        OffT elo = 0;
+        if (active) {
+          const int64_t r0 = (int64_t)a.g.R[r], r1 = (int64_t)a.g.R[r + 1];
+          const int64_t lo = max(r0, item_lo - (int64_t)r - 1);
+          const int64_t hi = min(r1, item_hi - (int64_t)r - 1);
+          cnt = hi > lo ? (uint32_t)(hi - lo) : 0u;
+          elo = (OffT)lo;
+          const int64_t rpos = (int64_t)r + r0;
+          n_rows += (rpos >= item_lo && rpos < item_hi) ? 1u : 0u;
+          n_edges += cnt;
+        }
+        const uint32_t incl = warp_inclusive_scan(cnt);
+        const uint32_t total = __shfl_sync(kFull, incl, 31);
+        if (total == 0) continue;
+        ex[lane] = incl - cnt;
+        lo_s[lane] = elo;
+        __syncwarp();
+        for (uint32_t base = 0; base < total; base += 32 * kUnroll) {
+          uint32_t t[kUnroll];
 #pragma unroll
-        for (int u = 0; u < kUnroll; ++u) {
-          const uint32_t i = base + u * 32 + lane;
-          t[u] = kFull;
-          if (i < total) {
-            const uint32_t j = owner_of(ex, i);
-            t[u] = __ldcs(a.g.C + lo_s[j] + (OffT)(i - ex[j]));
+          for (int u = 0; u < kUnroll; ++u) {
+            const uint32_t i = base + u * 32 + lane;
+            t[u] = kFull;
+            if (i < total) {
+              const uint32_t j = owner_of(ex, i);
+              t[u] = __ldcs(a.g.C + lo_s[j] + (OffT)(i - ex[j]));
+            }
+          }
+#pragma unroll
+          for (int u = 0; u < kUnroll; ++u) {
+            const uint32_t tword = t[u] == kFull ? kFull : (t[u] >> 5);
+            const uint32_t tbit = t[u] == kFull ? 0u : (1u << (t[u] & 31u));
+            bool head;
+            const uint32_t rm = run_mask(tword, &head);
+            const uint32_t bits = __reduce_or_sync(rm, tbit);
+            if (head && tword != kFull) atomicOr(a.wr + tword, bits);
           }
         }
-#pragma unroll
-        for (int u = 0; u < kUnroll; ++u) {
-          const uint32_t tword = t[u] == kFull ? kFull : (t[u] >> 5);
-          const uint32_t tbit = t[u] == kFull ? 0u : (1u << (t[u] & 31u));
-          bool head;
-          const uint32_t rm = run_mask(tword, &head);
-          const uint32_t bits = __reduce_or_sync(rm, tbit);
-          if (head && tword != kFull) atomicOr(a.wr + tword, bits);
-        }
+        __syncwarp();
       }
-      __syncwarp();
     }
   }
   n_rows = __reduce_add_sync(kFull, n_rows);
