@@ -56,7 +56,7 @@ UNIT = "GTEPS"
 REF_LIB = os.path.join(ROOT, "oracle", "_ref", "libref_harness.so")
 # kites_run_opts.strategy values (include/kites_b200.h).
 STRATEGIES = {"plain": 0, "auto": 1, "push": 2, "pull_all": 3, "tpv1": 4, "tpv4": 5,
-              "tpv8": 6, "tpv32": 7, "pull_changed": 8}
+              "tpv8": 6, "tpv32": 7, "pull_changed": 8, "mip": 9}
 
 
 def parse():
@@ -77,9 +77,9 @@ def parse():
                          "--mode batch: learned + batched); plain = the fixed plain kernel (the "
                          "default of --mode single); batch mode takes plain, auto, push, "
                          "pull_all and pull_changed")
-    ap.add_argument("--batch-gather", default="loads", choices=["loads", "tma"],
-                    help="how the batched pull fetches source rows: register loads or "
-                         "TMA tile::gather4 copies")
+    ap.add_argument("--batch-gather", default="async", choices=["loads", "tma", "async"],
+                    help="how the batched pull fetches source rows: register loads, "
+                         "TMA tile::gather4 copies, or cp.async copies into shared memory")
     ap.add_argument("--host-loop", action="store_true",
                     help="iterate from the host instead of the CUDA-graph device loop "
                          "(for kernel profilers)")
@@ -102,6 +102,11 @@ def parse():
     ap.add_argument("--batch-selector", default=None,
                     help="load the batched selector's weights from this file (1628 float32) "
                          "instead of the compiled-in default")
+    ap.add_argument("--mip-block", type=int, default=4096,
+                    help="--mode single --strategy mip (or a coarse class of MIP, "
+                         "--coarse mip): vertices per block of the block map")
+    ap.add_argument("--coarse", default="pull_all", choices=["pull_all", "mip"],
+                    help="single-source AUTO: what the selector's coarse class runs")
     ap.add_argument("--margin", type=float, default=None,
                     help="AUTO: the selector's fallback margin (kites_run_opts."
                          "selector_margin) instead of the library default")
@@ -418,7 +423,11 @@ def run_ours(args):
     if args.batch_selector:
         eng.selector_load_batch(np.fromfile(args.batch_selector, dtype="<f4"))
     g = capi.Graph(eng, R, C, E)
-    g.set_batch_gather(1 if args.batch_gather == "tma" else 0)
+    g.set_batch_gather({"loads": 0, "tma": 1, "async": 2}[args.batch_gather])
+    if args.mode == "single" and (args.strategy == "mip" or args.coarse == "mip"):
+        g.build_mipmap(args.mip_block)
+        if args.coarse == "mip":
+            g.set_coarse(capi.STRATEGY_MIP)
     stream = torch.cuda.ExternalStream(g.device_view().stream, device=device)
     srcs = pick_sources(outdeg, args.sources, args.seed, offset=rank)
     K = args.batch
@@ -433,7 +442,8 @@ def run_ours(args):
         r = g.autotune(srcs[:8], batch=K if args.mode == "batch" else 16)
         tuned = {"batch_chunk_items": int(r.batch_chunk_items),
                  "dense_edges": int(r.dense_edges), "dense_rows": int(r.dense_rows),
-                 "tpv_strategy": int(r.tpv_strategy), "trials": int(r.trials)}
+                 "tpv_strategy": int(r.tpv_strategy), "coarse_strategy": int(r.coarse_strategy),
+                 "trials": int(r.trials)}
     loop = 0 if args.host_loop else 1
     bopts = capi.default_opts(device_loop=loop, strategy=STRATEGIES[args.strategy])
     sopts = capi.default_opts(device_loop=loop, strategy=STRATEGIES[args.strategy])
@@ -582,7 +592,8 @@ def run_ours(args):
     # DRAM bytes per launch of the batched pull, from the ncu summary of the
     # same workload (one capture of every launch of a step), when there is one.
     traffic = None
-    prof = os.path.join(ROOT, "profiles", f"k_pull_batch_K{K}_rmat{args.scale}_traffic.md")
+    kname = "k_pull_batch_async" if args.batch_gather == "async" else "k_pull_batch"
+    prof = os.path.join(ROOT, "profiles", f"{kname}_K{K}_rmat{args.scale}_traffic.md")
     if args.mode == "batch" and os.path.exists(prof):
         import re
         hit = re.search(r"DRAM bytes per launch \(read \+ write, mean\): ([0-9]+)",
@@ -711,7 +722,8 @@ def run_ours(args):
             else None,
             "roofline": ({"bound": "hbm", "achieved": b_ach, "peak": peak, "unit": "GB/s",
                           "frac": b_ach / peak, "traffic": traffic,
-                          "kernel": f"k_pull_batch<SSSP,K={K}>",
+                          "kernel": (f"k_pull_batch_async<SSSP,K={K}>" if args.batch_gather == "async"
+                                     else f"k_pull_batch<SSSP,K={K}>"),
                           "launches": b_launch, "peak_source": src_note}
                          if b_ach is not None else
                          {"bound": "hbm", "achieved": p_ach, "peak": peak, "unit": "GB/s",

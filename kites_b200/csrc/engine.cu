@@ -15,6 +15,7 @@
 #include "engine.cuh"
 #include "kernels.cuh"
 #include "kernels_batch.cuh"
+#include "kernels_batch_async.cuh"
 #include "kernels_batch_tma.cuh"
 #include "kernels_mip.cuh"
 #include "kernels_pr.cuh"
@@ -460,7 +461,25 @@ struct batch_state {
   int grid;
   bool tma;       // TMA row gathers (g->dmap describes D)
   int tma_grid;
+  bool async;     // row gathers as cp.async copies into shared memory
+  int async_grid;
 };
+
+// Grid of k_pull_batch_async: as many CTAs as its shared memory and
+// registers let reside, capped by the chunk count.
+template <int OP, typename OffT, int K>
+int size_async_pull(kites_graph *g, int *out) {
+  const int smem = (int)async_batch_smem_bytes();
+  KITES_CUDA_TRY(cudaFuncSetAttribute(k_pull_batch_async<OP, OffT, K>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  int per_sm = 0;
+  KITES_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+      &per_sm, k_pull_batch_async<OP, OffT, K>, kBlock, smem));
+  const uint64_t cap = (uint64_t)std::max(per_sm, 1) * g->eng->sm_count;
+  const uint64_t want = (g->nchunks_batch + kWarpsPerBlock - 1) / kWarpsPerBlock;
+  *out = (int)std::max<uint64_t>(1, std::min(want, cap));
+  return KITES_OK;
+}
 
 template <int OP, typename OffT, int K>
 int launch_batch_iteration(kites_graph *g, const batch_state &b, int parity,
@@ -484,7 +503,10 @@ int launch_batch_iteration(kites_graph *g, const batch_state &b, int parity,
   }
   if (!launched) {
     pull_batch_args<OffT> pa{gb, (const uint32_t *)g->E, b.D, rd, chg, g->ctr};
-    k_pull_batch<OP, OffT, K><<<b.grid, kBlock, 0, s>>>(pa);
+    if (b.async)
+      k_pull_batch_async<OP, OffT, K><<<b.async_grid, kBlock, async_batch_smem_bytes(), s>>>(pa);
+    else
+      k_pull_batch<OP, OffT, K><<<b.grid, kBlock, 0, s>>>(pa);
   }
   if (time_pull) KITES_CUDA_TRY(cudaEventRecord(g->eng->kev1, s));
   launch_expand<OffT>(g, b.actR, b.actC, b.act_chunks, b.act_nchunks, true, b.act_rows,
@@ -1333,7 +1355,8 @@ int prepare_batch(kites_graph *g, uint32_t K, uint32_t items, batch_state *b) {
     b->act_nchunks = g->nchunks_out; b->act_rows = g->n; b->act_edges = g->m;
   }
   b->D = g->batchD;
-  b->tma = g->batch_gather != 0 && encode_batch_map(g, K);
+  b->tma = g->batch_gather == 1 && encode_batch_map(g, K);
+  b->async = g->batch_gather == 2;
   return KITES_OK;
 }
 
@@ -1410,6 +1433,7 @@ int run_batch(kites_graph *g, const uint32_t *sources, uint32_t *dist_out,
   } else {
     b.tma = false;
   }
+  if (b.async) KITES_TRY((size_async_pull<OP, OffT, K>(g, &b.async_grid)));
   KITES_CUDA_TRY(cudaMemcpyAsync(g->d_sources, sources, K * 4, cudaMemcpyDefault, s));
   k_fill_u32<<<grid_for(g->n * K), 256, 0, s>>>(b.D, g->n * K, kInf);
   KITES_CUDA_TRY(cudaMemsetAsync(b.bits, 0, 4 * b.nwords * 4, s));
@@ -1507,6 +1531,7 @@ struct batch_flex {
   const uint32_t *out_chunks;
   uint64_t out_nchunks;
   int pull_grid, mpull_grid, push_grid;
+  int async_grid;       // batch_gather 2: grid of k_pull_batch_async, else 0
 };
 
 // Selector class -> batched strategy.
@@ -1578,6 +1603,9 @@ int size_batch_flex_grids(kites_graph *g, batch_flex *f) {
   KITES_TRY(grid(k_pull_batch<OP, OffT, K, false>, g->nchunks_batch, &f->pull_grid));
   KITES_TRY(grid(k_pull_batch<OP, OffT, K, true>, g->nchunks_batch, &f->mpull_grid));
   KITES_TRY(grid(k_push_batch<OP, OffT, K>, f->out_nchunks, &f->push_grid));
+  f->async_grid = 0;
+  if (g->batch_gather == 2)
+    KITES_TRY((size_async_pull<OP, OffT, K>(g, &f->async_grid)));
   return KITES_OK;
 }
 
@@ -1598,7 +1626,10 @@ int launch_batch_strategy(kites_graph *g, const batch_flex &f, int strategy, int
       launch_expand<OffT>(g, f.actR, f.actC, f.act_chunks, f.act_nchunks, true, f.act_rows,
                           f.act_edges, Uc, f.A, 0u, launches);
       pull_batch_args<OffT> pa{gb, (const uint32_t *)g->E, f.D, f.A, Un, g->ctr, Mc, Mn};
-      if (strategy == KITES_STRATEGY_PLAIN)
+      if (strategy == KITES_STRATEGY_PLAIN && f.async_grid)
+        k_pull_batch_async<OP, OffT, K><<<f.async_grid, kBlock, async_batch_smem_bytes(), s>>>(
+            pa);
+      else if (strategy == KITES_STRATEGY_PLAIN)
         k_pull_batch<OP, OffT, K, false><<<f.pull_grid, kBlock, 0, s>>>(pa);
       else
         k_pull_batch<OP, OffT, K, true><<<f.mpull_grid, kBlock, 0, s>>>(pa);
@@ -1608,7 +1639,11 @@ int launch_batch_strategy(kites_graph *g, const batch_flex &f, int strategy, int
       // Every row over whole source rows: no activation pass, and exact
       // without the changed-sector invariant (every in-edge is folded).
       pull_batch_args<OffT> pa{gb, (const uint32_t *)g->E, f.D, nullptr, Un, g->ctr, Mc, Mn};
-      k_pull_batch<OP, OffT, K, false><<<f.pull_grid, kBlock, 0, s>>>(pa);
+      if (f.async_grid)
+        k_pull_batch_async<OP, OffT, K><<<f.async_grid, kBlock, async_batch_smem_bytes(), s>>>(
+            pa);
+      else
+        k_pull_batch<OP, OffT, K, false><<<f.pull_grid, kBlock, 0, s>>>(pa);
       break;
     }
     case KITES_STRATEGY_PUSH: {
@@ -3014,7 +3049,7 @@ extern "C" int kites_autotune(kites_engine *eng, kites_graph *g, int op, const u
 extern "C" int kites_graph_set_batch_gather(kites_graph *g, int mode) {
   clear_error();
   if (!g) return fail(KITES_ERR_INVALID, "null graph");
-  if (mode != 0 && mode != 1) return fail(KITES_ERR_INVALID, "batch gather mode is 0 or 1");
+  if (mode < 0 || mode > 2) return fail(KITES_ERR_INVALID, "batch gather mode is 0, 1 or 2");
   KITES_TRY(set_device(g->eng));
   KITES_CUDA_TRY(cudaStreamSynchronize(g->eng->stream));
   g->batch_gather = mode;

@@ -26,9 +26,19 @@ def test_strategy_table_matches_the_abi():
                                 "push": capi.STRATEGY_PUSH, "pull_all": capi.STRATEGY_PULL_ALL,
                                 "tpv1": capi.STRATEGY_TPV1, "tpv4": capi.STRATEGY_TPV4,
                                 "tpv8": capi.STRATEGY_TPV8, "tpv32": capi.STRATEGY_TPV32,
-                                "pull_changed": capi.STRATEGY_PULL_CHANGED}
+                                "pull_changed": capi.STRATEGY_PULL_CHANGED,
+                                "mip": capi.STRATEGY_MIP}
 
 
 @pytest.mark.parametrize("strategy", ["plain", "auto", "push", "pull_all", "pull_changed"])
 def test_batch_strategies_parse(monkeypatch, strategy):
     assert parse(monkeypatch, "--strategy", strategy).strategy == strategy
+
+
+def test_gather_margin_and_coarse_options(monkeypatch):
+    a = parse(monkeypatch, "--batch-gather", "async", "--margin", "0.05")
+    assert a.batch_gather == "async" and abs(a.margin - 0.05) < 1e-12
+    a = parse(monkeypatch, "--mode", "single", "--strategy", "mip", "--mip-block", "1024")
+    assert a.strategy == "mip" and a.mip_block == 1024 and a.coarse == "pull_all"
+    assert parse(monkeypatch, "--mode", "single", "--strategy", "auto",
+                 "--coarse", "mip").coarse == "mip"

@@ -243,8 +243,8 @@ def test_repeated_runs_and_pool_reuse(engine, cfg1_edges):
 @pytest.mark.parametrize("k", [32, 64, 128, 256])
 @pytest.mark.parametrize("device_loop", [0, 1])
 def test_batch_gather_modes_agree(engine, k, device_loop):
-    """TMA row gathers (gather mode 1, K >= 32) and register loads (mode 0,
-    the default) give the same V x K distances, run after run, on one graph."""
+    """TMA row gathers (gather mode 1, K >= 32) and register loads (mode 0)
+    give the same V x K distances, run after run, on one graph."""
     n = 1 << 14
     s, d, w = capi.gen_rmat(14, 16 << 14, seed=31)
     R, C, E = capi.csc_from_edges(n, s, d, w)
@@ -263,6 +263,47 @@ def test_batch_gather_modes_agree(engine, k, device_loop):
     np.testing.assert_array_equal(tma[:, k // 2], single)
     assert st.iterations > 1
     g.close()
+
+
+@pytest.mark.parametrize("k", [16, 32, 64, 128, 256])
+@pytest.mark.parametrize("strategy", [capi.STRATEGY_PLAIN, capi.STRATEGY_AUTO,
+                                      capi.STRATEGY_PULL_ALL])
+def test_batch_async_gathers_agree(engine, k, strategy):
+    """cp.async row copies into shared memory (gather mode 2) give the V x K
+    distances of the register loads (mode 0), in the fixed batched loop and in
+    the batched strategies' unmasked pulls, and each column is the
+    single-source result."""
+    n = 1 << 14
+    s, d, w = capi.gen_rmat(14, 16 << 14, seed=33)
+    R, C, E = capi.csc_from_edges(n, s, d, w)
+    g = capi.Graph(engine, R, C, E)
+    try:
+        srcs = np.random.default_rng(300 + k).choice(n, size=k, replace=False).astype(np.uint32)
+        o = capi.default_opts(strategy=strategy)
+        g.set_batch_gather(0)
+        loads, _ = g.sssp_batch(srcs, opts=o)
+        g.set_batch_gather(2)
+        cpa, st = g.sssp_batch(srcs, opts=o)
+        again, _ = g.sssp_batch(srcs, opts=o)
+        np.testing.assert_array_equal(cpa, loads)
+        np.testing.assert_array_equal(again, loads)
+        for j in (0, k // 2, k - 1):
+            np.testing.assert_array_equal(cpa[:, j], g.sssp(int(srcs[j]))[0])
+        assert st.iterations > 1
+    finally:
+        g.close()
+
+
+def test_batch_gather_rejects_unknown_modes(engine):
+    s, d, w = capi.gen_er(1000, 4000, seed=2)
+    R, C, E = capi.csc_from_edges(1000, s, d, w)
+    g = capi.Graph(engine, R, C, E)
+    try:
+        for mode in (-1, 3):
+            with pytest.raises(capi.KitesError):
+                g.set_batch_gather(mode)
+    finally:
+        g.close()
 
 
 @pytest.mark.parametrize("k", [16, 32, 64, 128, 256])
@@ -336,9 +377,13 @@ def test_uint64_offsets_give_the_same_results(engine, offsets64):
         np.testing.assert_array_equal(g.sssp(7, opts=o)[0], g32.sssp(7)[0])
     np.testing.assert_array_equal(g.sssp(7, op=capi.OP_BFS)[0], g32.sssp(7, op=capi.OP_BFS)[0])
     srcs = np.arange(64, dtype=np.uint32) * 101
-    for mode in (0, 1):
+    for mode in (0, 1, 2):
         g.set_batch_gather(mode)
         np.testing.assert_array_equal(g.sssp_batch(srcs)[0], g32.sssp_batch(srcs)[0])
+    g.set_batch_gather(2)
+    np.testing.assert_array_equal(
+        g.sssp_batch(srcs, opts=capi.default_opts(strategy=capi.STRATEGY_AUTO))[0],
+        g32.sssp_batch(srcs)[0])
     pr, _ = g.pagerank(n_real=n)
     pr32, _ = g32.pagerank(n_real=n)
     assert np.abs(pr.astype(np.float64) - pr32).sum() / np.abs(pr32).sum() < 1e-6
