@@ -467,14 +467,14 @@ struct batch_state {
 
 // Grid of k_pull_batch_async: as many CTAs as its shared memory and
 // registers let reside, capped by the chunk count.
-template <int OP, typename OffT, int K>
+template <int OP, typename OffT, int K, bool kMasked = false>
 int size_async_pull(kites_graph *g, int *out) {
   const int smem = (int)async_batch_smem_bytes();
-  KITES_CUDA_TRY(cudaFuncSetAttribute(k_pull_batch_async<OP, OffT, K>,
+  KITES_CUDA_TRY(cudaFuncSetAttribute(k_pull_batch_async<OP, OffT, K, kMasked>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   int per_sm = 0;
   KITES_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-      &per_sm, k_pull_batch_async<OP, OffT, K>, kBlock, smem));
+      &per_sm, k_pull_batch_async<OP, OffT, K, kMasked>, kBlock, smem));
   const uint64_t cap = (uint64_t)std::max(per_sm, 1) * g->eng->sm_count;
   const uint64_t want = (g->nchunks_batch + kWarpsPerBlock - 1) / kWarpsPerBlock;
   *out = (int)std::max<uint64_t>(1, std::min(want, cap));
@@ -1532,6 +1532,7 @@ struct batch_flex {
   uint64_t out_nchunks;
   int pull_grid, mpull_grid, push_grid;
   int async_grid;       // batch_gather 2: grid of k_pull_batch_async, else 0
+  int async_mgrid;      // the same for its masked form
 };
 
 // Selector class -> batched strategy.
@@ -1603,9 +1604,11 @@ int size_batch_flex_grids(kites_graph *g, batch_flex *f) {
   KITES_TRY(grid(k_pull_batch<OP, OffT, K, false>, g->nchunks_batch, &f->pull_grid));
   KITES_TRY(grid(k_pull_batch<OP, OffT, K, true>, g->nchunks_batch, &f->mpull_grid));
   KITES_TRY(grid(k_push_batch<OP, OffT, K>, f->out_nchunks, &f->push_grid));
-  f->async_grid = 0;
-  if (g->batch_gather == 2)
+  f->async_grid = f->async_mgrid = 0;
+  if (g->batch_gather == 2) {
     KITES_TRY((size_async_pull<OP, OffT, K>(g, &f->async_grid)));
+    KITES_TRY((size_async_pull<OP, OffT, K, true>(g, &f->async_mgrid)));
+  }
   return KITES_OK;
 }
 
@@ -1631,6 +1634,9 @@ int launch_batch_strategy(kites_graph *g, const batch_flex &f, int strategy, int
             pa);
       else if (strategy == KITES_STRATEGY_PLAIN)
         k_pull_batch<OP, OffT, K, false><<<f.pull_grid, kBlock, 0, s>>>(pa);
+      else if (f.async_mgrid)
+        k_pull_batch_async<OP, OffT, K, true>
+            <<<f.async_mgrid, kBlock, async_batch_smem_bytes(), s>>>(pa);
       else
         k_pull_batch<OP, OffT, K, true><<<f.mpull_grid, kBlock, 0, s>>>(pa);
       break;

@@ -4,8 +4,9 @@
 // register, so each lane group keeps kAsyncRows source rows in flight where
 // the register version (k_pull_batch) keeps four at 64 registers and
 // spills.  The work split, folds, updates and changed-sector marks are
-// k_pull_batch's unmasked path; kites_graph_set_batch_gather(g, 2) selects
-// it.
+// k_pull_batch's (unmasked, and masked: only the changed sectors of each
+// in-neighbour's row, the live in-edges of a tile packed first);
+// kites_graph_set_batch_gather(g, 2) selects it.
 //
 // Each lane copies and later reads back only its own 32 bytes of each row
 // slot, so a lane waits for its own copies (cp.async.wait_all) and no
@@ -41,12 +42,13 @@ __device__ __forceinline__ void smem_row8(const uint4 *smem, uint32_t (&x)[8]) {
   x[4] = q.x; x[5] = q.y; x[6] = q.z; x[7] = q.w;
 }
 
-template <int OP, typename OffT, int K>
+template <int OP, typename OffT, int K, bool kMasked = false>
 __global__ void __launch_bounds__(kBlock, 3) k_pull_batch_async(pull_batch_args<OffT> a) {
   if (a.ctr->done) return;
   using S = batch_shape<K>;
   static_assert(S::VPL == 8, "one 32-byte sector per lane");
   extern __shared__ uint4 s_rows[];   // [warp][slot][lane][2]
+  __shared__ uint8_t s_slot[kWarpsPerBlock][32];   // masked: lane of the j-th live edge
   const uint32_t lane = lane_id(), wib = threadIdx.x >> 5;
   const uint32_t sub = lane / S::LPE, kl = lane % S::LPE;
   // This lane's slot r: my + r * 64 (32 lanes x 2 uint4 per slot).
@@ -65,7 +67,7 @@ __global__ void __launch_bounds__(kBlock, 3) k_pull_batch_async(pull_batch_args<
       if (vb < v_first) mask &= kFull << (uint32_t)(v_first - vb);
       if (v_last - vb < 31) mask &= kFull >> (31u - (uint32_t)(v_last - vb));
       uint32_t upd_bits = 0;
-      if constexpr (S::EPW >= 2) {
+      if constexpr (!kMasked && S::EPW >= 2) {
         // Short rows (at most kShortRow in-edges in this chunk): one lane
         // group each, kAsyncRows gathers in flight per group.
         int64_t my_lo = 0, my_hi = 0;
@@ -164,35 +166,57 @@ __global__ void __launch_bounds__(kBlock, 3) k_pull_batch_async(pull_batch_args<
         uint32_t acc[S::VPL];
 #pragma unroll
         for (int q = 0; q < S::VPL; ++q) acc[q] = kInf;
+        bool row_live = !kMasked;
         for (int64_t tile = lo; tile < hi; tile += 32) {
           const int64_t t = tile + lane;
-          const uint32_t ntile = (uint32_t)min((int64_t)32, hi - tile);
-          uint32_t cC = 0, cE = 0;
+          uint32_t ntile = (uint32_t)min((int64_t)32, hi - tile);
+          uint32_t cC = 0, cE = 0, cM = 0;
           if (t < hi) {
             cC = __ldcs(a.g.C + t);
             if (op_reads_weights<OP>()) cE = __ldcs(a.E + t);
           }
+          if constexpr (kMasked) {
+            cM = t < hi ? a.Mprev[cC] : 0u;
+            const uint32_t live = __ballot_sync(kFull, cM != 0u);
+            if (cM) s_slot[wib][__popc(live & ((1u << lane) - 1u))] = (uint8_t)lane;
+            __syncwarp();
+            ntile = __popc(live);
+            row_live = row_live || live != 0u;
+          }
           for (uint32_t jj = 0; jj < ntile; jj += S::EPW * kAsyncRows) {
             uint32_t wq[kAsyncRows];
+            bool tk[kAsyncRows];
 #pragma unroll
             for (int r = 0; r < kAsyncRows; ++r) {
               const uint32_t j = jj + r * S::EPW + sub;
-              // Every lane takes part in every shuffle (full mask).
-              const uint32_t u = __shfl_sync(kFull, cC, j & 31u);
-              wq[r] = __shfl_sync(kFull, cE, j & 31u);
-              if (j < ntile) cp_async_row8(my + r * 64, a.D + (uint64_t)u * K + kl * S::VPL);
+              const uint32_t src = kMasked ? (j < ntile ? (uint32_t)s_slot[wib][j] : 0u)
+                                           : (j & 31u);
+              // Every lane takes part in every shuffle (full mask), whether
+              // or not its slot gathers anything.
+              const uint32_t u = __shfl_sync(kFull, cC, src);
+              wq[r] = __shfl_sync(kFull, cE, src);
+              const uint32_t mu = kMasked ? __shfl_sync(kFull, cM, src) : kFull;
+              bool take = j < ntile && ((mu >> kl) & 1u);
+              if (kMasked && take && u >= a.g.n_rows) {  // never index with an id out of range
+                raise_error(a.ctr, kErrIndex);
+                take = false;
+              }
+              tk[r] = take;
+              if (take) cp_async_row8(my + r * 64, a.D + (uint64_t)u * K + kl * S::VPL);
             }
             cp_async_wait_all();
 #pragma unroll
             for (int r = 0; r < kAsyncRows; ++r) {
-              if (jj + r * S::EPW + sub >= ntile) continue;
+              if (!tk[r]) continue;
               uint32_t x[S::VPL];
               smem_row8(my + r * 64, x);
 #pragma unroll
               for (int q = 0; q < S::VPL; ++q) acc[q] = min(acc[q], nbr_comp<OP>(x[q], wq[r]));
             }
           }
+          if constexpr (kMasked) __syncwarp();  // s_slot is rewritten by the next tile
         }
+        if (!row_live) continue;  // masked: no in-neighbour changed
 #pragma unroll
         for (int d = S::LPE; d < 32; d <<= 1) {
 #pragma unroll
