@@ -26,8 +26,9 @@ a 268M-edge graph is built once per machine.
 --impl reference times farkhor/KiTES's own CPU vertex-centric loop
 (kites::sanity_check, compiled from the reference headers into
 oracle/_ref/libref_harness.so) on the same graph: each step is the SSSP of
-one of the workload's sources, and the steps run side by side, one per host
-thread.  That process reads or generates the graph through the oracle only
+one of the workload's sources (or of threads // K of them, when the K timed
+steps would leave host threads idle), and the sources run side by side, one
+per host thread.  That process reads or generates the graph through the oracle only
 (oracle/csc_file.py, the oracle's own generator) and never loads the
 library under test.
 """
@@ -341,9 +342,10 @@ def time_reference(lib, n, m, R32, C, E, outdeg, sources, threads, want_dist=Fal
     return secs, reached, dist
 
 
-def ref_sample_text(n, m, k, threads):
+def ref_sample_text(n, m, k, threads, per_step=1):
+    step = "one source per step" if per_step == 1 else f"{per_step} sources per step"
     return (f"SSSP from {k} of the workload's sources on the same R-MAT graph ({n} vertices, "
-            f"{m} edges), one source per step, by farkhor/KiTES's own kites::sanity_check loop "
+            f"{m} edges), {step}, by farkhor/KiTES's own kites::sanity_check loop "
             f"(single-threaded per source), {threads} sources side by side on {threads} host "
             f"threads")
 
@@ -366,27 +368,31 @@ def run_reference(args):
     R32 = R.astype(np.uint32)
     del R
     threads = host_threads(args.ref_threads)
-    srcs = pick_sources(outdeg, max(args.sources, args.steps + args.warmup), args.seed)
-    # Warm-up: W steps (sources) side by side, untimed; then exactly K steps,
-    # the first K of the workload's sources, timed from the first loop's
-    # start to the last one's end.
+    # A step is a sample of the workload's sources: one source, or as many as
+    # let the K timed steps fill every host thread in one wave.
+    per_step = max(1, threads // max(1, args.steps))
+    k = args.steps * per_step
+    srcs = pick_sources(outdeg, max(args.sources, k + args.warmup), args.seed)
+    # Warm-up: W sources side by side, untimed; then exactly K steps, the
+    # first K x per_step of the workload's sources, timed from the first
+    # loop's start to the last one's end.
     if args.warmup:
-        time_reference(lib, n, m, R32, C, E, outdeg, srcs[args.steps:args.steps + args.warmup],
-                       threads)
-    secs, reached, _ = time_reference(lib, n, m, R32, C, E, outdeg, srcs[:args.steps], threads)
+        time_reference(lib, n, m, R32, C, E, outdeg, srcs[k:k + args.warmup], threads)
+    secs, reached, _ = time_reference(lib, n, m, R32, C, E, outdeg, srcs[:k], threads)
     value = float(reached.sum()) / secs / 1e9
+    used = min(threads, k)
     config = dict(workload_config(args), mode="reference CPU loop", batch=1,
-                  sources_per_step=1, strategy="kites::sanity_check (Gauss-Seidel sweep)",
-                  threads=min(threads, args.steps), batch_gather=None)
+                  sources_per_step=per_step, strategy="kites::sanity_check (Gauss-Seidel sweep)",
+                  threads=used, batch_gather=None)
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "metric_detail": METRIC_DETAIL, "value": value, "unit": UNIT,
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * secs / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
         "config": config,
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": min(threads, args.steps),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": used,
                          "kind": "reference",
-                         "sample": ref_sample_text(n, m, args.steps, min(threads, args.steps))},
+                         "sample": ref_sample_text(n, m, k, used, per_step)},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }))
