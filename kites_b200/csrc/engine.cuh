@@ -107,7 +107,8 @@ struct kites_graph {
   uint32_t *d_sources = nullptr;     // 256 source slots
   // TMA view of batchD (K-wide rows) for the gather kernel; batch_gather:
   // 2 = cp.async row copies into shared memory (default: R-MAT scale 24,
-  // learned + batched 291.0 against 254.3 GTEPS with register loads),
+  // learned + batched 291.0 against 254.3 GTEPS with register loads, 305
+  // with six rows in flight per lane group at four CTAs per SM),
   // 1 = TMA row gathers when K >= 32, 0 = register loads.
   CUtensorMap dmap;
   const void *dmap_ptr = nullptr;
