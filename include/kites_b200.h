@@ -405,8 +405,8 @@ int kites_autotune(kites_engine *eng, kites_graph *g, int op, const uint32_t *so
 int kites_graph_set_density(kites_graph *g, uint64_t dense_edges, uint64_t dense_rows);
 /* How kites_sssp_batch fetches the K-wide source rows (no counterpart in the
  * reference, whose kernels run one source at a time): 2 (default) = per-lane
- * cp.async copies into shared memory (the fixed batched loop and the
- * unmasked pulls of the batched strategies), 0 = 256-bit register loads,
+ * cp.async copies into shared memory (the fixed batched loop, and the pulls
+ * and the push of the batched strategies), 0 = 256-bit register loads,
  * 1 = TMA tile::gather4 copies into shared memory when K >= 32 (the fixed
  * batched loop only).  All give identical results. */
 int kites_graph_set_batch_gather(kites_graph *g, int mode);

@@ -1533,6 +1533,7 @@ struct batch_flex {
   int pull_grid, mpull_grid, push_grid;
   int async_grid;       // batch_gather 2: grid of k_pull_batch_async, else 0
   int async_mgrid;      // the same for its masked form
+  int async_push_grid;  // batch_gather 2: grid of k_push_batch_async, else 0
 };
 
 // Selector class -> batched strategy.
@@ -1604,10 +1605,19 @@ int size_batch_flex_grids(kites_graph *g, batch_flex *f) {
   KITES_TRY(grid(k_pull_batch<OP, OffT, K, false>, g->nchunks_batch, &f->pull_grid));
   KITES_TRY(grid(k_pull_batch<OP, OffT, K, true>, g->nchunks_batch, &f->mpull_grid));
   KITES_TRY(grid(k_push_batch<OP, OffT, K>, f->out_nchunks, &f->push_grid));
-  f->async_grid = f->async_mgrid = 0;
+  f->async_grid = f->async_mgrid = f->async_push_grid = 0;
   if (g->batch_gather == 2) {
     KITES_TRY((size_async_pull<OP, OffT, K>(g, &f->async_grid)));
     KITES_TRY((size_async_pull<OP, OffT, K, true>(g, &f->async_mgrid)));
+    const int smem = (int)async_push_smem_bytes();
+    KITES_CUDA_TRY(cudaFuncSetAttribute(k_push_batch_async<OP, OffT, K>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    int per_sm = 0;
+    KITES_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &per_sm, k_push_batch_async<OP, OffT, K>, kBlock, smem));
+    const uint64_t cap = (uint64_t)std::max(per_sm, 1) * sms;
+    const uint64_t want = (f->out_nchunks + kWarpsPerBlock - 1) / kWarpsPerBlock;
+    f->async_push_grid = (int)std::max<uint64_t>(1, std::min(want, cap));
   }
   return KITES_OK;
 }
@@ -1656,7 +1666,11 @@ int launch_batch_strategy(kites_graph *g, const batch_flex &f, int strategy, int
       chunk_geom<OffT> go{(const OffT *)f.outR, g->outC, f.out_chunks, f.out_nchunks,
                           g->n, g->n + g->m, g->chunk_items};
       push_batch_args<OffT> pa{go, g->outE, f.D, Uc, Mc, Un, Mn, g->ctr};
-      k_push_batch<OP, OffT, K><<<f.push_grid, kBlock, 0, s>>>(pa);
+      if (f.async_push_grid)
+        k_push_batch_async<OP, OffT, K>
+            <<<f.async_push_grid, kBlock, async_push_smem_bytes(), s>>>(pa);
+      else
+        k_push_batch<OP, OffT, K><<<f.push_grid, kBlock, 0, s>>>(pa);
       break;
     }
     default:

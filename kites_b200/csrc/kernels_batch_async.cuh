@@ -263,4 +263,153 @@ __global__ void __launch_bounds__(kBlock, 4) k_pull_batch_async(pull_batch_args<
   }
 }
 
+// ---- masked push with asynchronous copies ------------------------------------
+
+// Out-edges in flight per lane group in k_push_batch_async.
+constexpr int kPushRows = 3;
+
+// Dynamic shared memory per CTA: per warp, per out-edge slot, the source's
+// and the target's 32 bytes for each lane.
+constexpr size_t async_push_smem_bytes() {
+  return (size_t)kWarpsPerBlock * kPushRows * 2 * 32 * 32;
+}
+
+// The source row sector through L1 (the push reads one source row once per
+// out-edge, so repeats hit there).
+__device__ __forceinline__ void cp_async_row8_l1(uint4 *smem, const uint32_t *gmem) {
+  const uint32_t s = (uint32_t)__cvta_generic_to_shared(smem);
+  asm volatile(
+      "cp.async.ca.shared.global [%0], [%1], 16;\n\t"
+      "cp.async.ca.shared.global [%2], [%3], 16;" ::"r"(s),
+      "l"(gmem), "r"(s + 16u), "l"(gmem + 4)
+      : "memory");
+}
+
+// k_push_batch with kPushRows out-edges per lane group in flight: the
+// source's changed sectors and the target's current sectors of each edge are
+// copied into shared memory together (cp.async), then the edges are relaxed
+// one after another with atomicMin where the candidate beats the copy.  A
+// source lowered by an earlier edge of the same round is read before that
+// lowering; it is in the next changed set with those sectors marked, so its
+// out-edges are pushed again then (the masked push's invariant).
+template <int OP, typename OffT, int K>
+__global__ void __launch_bounds__(kBlock, 4) k_push_batch_async(push_batch_args<OffT> a) {
+  if (a.ctr->done) return;
+  using S = batch_shape<K>;
+  static_assert(S::VPL == 8, "one 32-byte sector per lane");
+  extern __shared__ uint4 s_push[];   // [warp][slot][source|target][lane][2]
+  __shared__ uint32_t s_ex[kWarpsPerBlock][32];
+  __shared__ OffT s_lo[kWarpsPerBlock][32];
+  const uint32_t lane = lane_id(), wib = threadIdx.x >> 5;
+  const uint32_t sub = lane / S::LPE, kl = lane % S::LPE;
+  uint32_t *ex = s_ex[wib];
+  OffT *lo_s = s_lo[wib];
+  // This lane's source slot r: my + r * 128; its target slot: my + r * 128 + 64.
+  uint4 *my = s_push + ((size_t)wib * kPushRows * 2 * 32 + lane) * 2;
+  unsigned long long n_rows = 0, n_edges = 0, n_chg = 0;
+  bool any = false;
+  const uint64_t stride = (uint64_t)gridDim.x * kWarpsPerBlock;
+  for (uint64_t ch = (uint64_t)blockIdx.x * kWarpsPerBlock + wib; ch < a.g.nchunks;
+       ch += stride) {
+    const int64_t item_lo = (int64_t)(ch * a.g.chunk_items);
+    const int64_t item_hi = min(item_lo + (int64_t)a.g.chunk_items, (int64_t)a.g.n_items);
+    const uint64_t r_first = a.g.chunk_v0[ch];
+    uint64_t r_last = a.g.chunk_v0[ch + 1];
+    if (r_last >= a.g.n_rows) r_last = a.g.n_rows - 1;
+    for (uint64_t rb = r_first & ~31ull; rb <= r_last; rb += 32) {
+      const uint32_t word = a.U[rb >> 5];
+      if (word == 0) continue;
+      const uint64_t r = rb + lane;
+      const bool active = r >= r_first && r <= r_last && ((word >> lane) & 1u);
+      uint32_t cnt = 0;
+      OffT elo = 0;
+      if (active) {
+        const int64_t r0 = (int64_t)a.g.R[r], r1 = (int64_t)a.g.R[r + 1];
+        const int64_t lo = max(r0, item_lo - (int64_t)r - 1);
+        const int64_t hi = min(r1, item_hi - (int64_t)r - 1);
+        cnt = hi > lo ? (uint32_t)(hi - lo) : 0u;
+        elo = (OffT)lo;
+        const int64_t rpos = (int64_t)r + r0;
+        n_rows += (rpos >= item_lo && rpos < item_hi) ? 1u : 0u;
+        n_edges += cnt;
+      }
+      const uint32_t incl = warp_inclusive_scan(cnt);
+      const uint32_t total = __shfl_sync(kFull, incl, 31);
+      if (total == 0) continue;
+      ex[lane] = incl - cnt;
+      lo_s[lane] = elo;
+      __syncwarp();
+      for (uint32_t base = 0; base < total; base += 32) {
+        // Lane i loads virtual out-edge base + i: target, weight, source row
+        // and the source's changed sectors.
+        const uint32_t i = base + lane;
+        uint32_t tv = 0, tw = 0, tr = 0, tm = 0;
+        if (i < total) {
+          const uint32_t j = owner_of(ex, i);
+          const OffT e = lo_s[j] + (OffT)(i - ex[j]);
+          tv = __ldcs(a.g.C + e);
+          if (op_reads_weights<OP>()) tw = __ldcs(a.outE + e);
+          tr = (uint32_t)(rb + j);
+          tm = a.Mprev[tr];
+        }
+        const uint32_t nwin = min(32u, total - base);
+        for (uint32_t s0 = 0; s0 < nwin; s0 += S::EPW * kPushRows) {
+          uint32_t vv[kPushRows], ww[kPushRows];
+          bool tk[kPushRows];
+#pragma unroll
+          for (int q = 0; q < kPushRows; ++q) {
+            const uint32_t idx = s0 + q * S::EPW + sub;
+            const uint32_t sl = idx & 31u;
+            // Every lane takes part in every shuffle (full mask).
+            vv[q] = __shfl_sync(kFull, tv, sl);
+            ww[q] = __shfl_sync(kFull, tw, sl);
+            const uint32_t u = __shfl_sync(kFull, tr, sl);
+            const uint32_t mu = __shfl_sync(kFull, tm, sl);
+            tk[q] = idx < nwin && ((mu >> kl) & 1u);
+            if (tk[q]) {
+              cp_async_row8_l1(my + q * 128, a.D + (uint64_t)u * K + kl * S::VPL);
+              cp_async_row8(my + q * 128 + 64, a.D + (uint64_t)vv[q] * K + kl * S::VPL);
+            }
+          }
+          cp_async_wait_all();
+#pragma unroll
+          for (int q = 0; q < kPushRows; ++q) {
+            bool lowered = false;
+            if (tk[q]) {
+              uint32_t du[S::VPL], cur[S::VPL];
+              smem_row8(my + q * 128, du);
+              smem_row8(my + q * 128 + 64, cur);
+              uint32_t *dv = a.D + (uint64_t)vv[q] * K + kl * S::VPL;
+#pragma unroll
+              for (int x = 0; x < S::VPL; ++x) {
+                const uint32_t nd = nbr_comp<OP>(du[x], ww[q]);
+                if (nd < cur[x] && nd < atomicMin(dv + x, nd)) lowered = true;
+              }
+            }
+            // The group's first lane publishes the sectors its lanes lowered.
+            const uint32_t gbits =
+                (__ballot_sync(kFull, lowered) >> (sub * S::LPE)) & S::kSectors;
+            if (gbits && kl == 0) {
+              atomicOr(a.Mnext + vv[q], gbits);
+              const uint32_t bit = 1u << (vv[q] & 31u);
+              if (!(atomicOr(a.chg + (vv[q] >> 5), bit) & bit)) ++n_chg;
+              any = true;
+            }
+          }
+        }
+      }
+      __syncwarp();
+    }
+  }
+  if (__any_sync(kFull, any) && lane == 0) a.ctr->update_flag = 1u;
+  n_rows = warp_sum_u64(n_rows);
+  n_edges = warp_sum_u64(n_edges);
+  n_chg = warp_sum_u64(n_chg);
+  if (lane == 0) {
+    if (n_rows) atomicAdd(&a.ctr->active, n_rows);
+    if (n_edges) atomicAdd(&a.ctr->edges, n_edges);
+    if (n_chg) atomicAdd(&a.ctr->changed, n_chg);
+  }
+}
+
 }  // namespace kites_internal

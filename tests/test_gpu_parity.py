@@ -267,12 +267,13 @@ def test_batch_gather_modes_agree(engine, k, device_loop):
 
 @pytest.mark.parametrize("k", [16, 32, 64, 128, 256])
 @pytest.mark.parametrize("strategy", [capi.STRATEGY_PLAIN, capi.STRATEGY_AUTO,
-                                      capi.STRATEGY_PULL_ALL, capi.STRATEGY_PULL_CHANGED])
+                                      capi.STRATEGY_PULL_ALL, capi.STRATEGY_PULL_CHANGED,
+                                      capi.STRATEGY_PUSH])
 def test_batch_async_gathers_agree(engine, k, strategy):
     """cp.async row copies into shared memory (gather mode 2) give the V x K
     distances of the register loads (mode 0), in the fixed batched loop and in
     the batched strategies' pulls (unmasked, and masked to the changed
-    sectors), and each column is the single-source result."""
+    sectors) and masked push, and each column is the single-source result."""
     n = 1 << 14
     s, d, w = capi.gen_rmat(14, 16 << 14, seed=33)
     R, C, E = capi.csc_from_edges(n, s, d, w)
